@@ -1,0 +1,195 @@
+/*
+ * isp_b200.h - the C ABI of the B200 image signal processor.
+ *
+ * A raw Bayer mosaic in, RGB out, with optional histograms and statistics,
+ * computed by sm_100a kernels bit for bit as the holoscan::isp CPU backend
+ * computes them. Plain C: pointers, sizes and PODs, no CUDA or C++ types, so
+ * that any language with a C FFI (ctypes, cgo, JNI, N-API) can bind it.
+ *
+ * Every entry point returns an isp_status (0 on success). On failure the
+ * message of the calling thread's last error is in isp_b200_last_error().
+ *
+ * Reference interfaces replaced (paths inside the holoscan-zozo-modules tree):
+ *   modules/isp/include/holoscan/isp/isp_params.hpp:21-198   enums, IspParams, views, layouts
+ *   modules/isp/include/holoscan/isp/isp_pipeline.hpp:39-74  class IspPipeline
+ *   modules/isp/src/isp_params.cpp:85-237                     validate_params, tone_lut,
+ *                                                             raw_row_bytes, validate_raw
+ */
+#ifndef ISP_B200_H_
+#define ISP_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ISP_B200_ABI_VERSION 1
+
+/* Status codes. ISP_EINVAL is std::invalid_argument in the reference façade
+ * (isp_pipeline.hpp:41-44), ISP_ECUDA its std::runtime_error from a CUDA failure. */
+typedef enum isp_status {
+  ISP_OK = 0,
+  ISP_EINVAL = 1,   /* A setting or a view is not usable. */
+  ISP_ECUDA = 2,    /* A CUDA call failed; isp_b200_last_cuda_error() has its code. */
+  ISP_ETIMEOUT = 3, /* A bounded wait ran out (device spin or host poll). */
+  ISP_EBUSY = 4,    /* Admission refused: the memory budget or the queue is full. */
+  ISP_ESTATE = 5    /* The call does not fit the object's state (e.g. closed server). */
+} isp_status;
+
+/* Enumerations, with the reference's numbering (isp_params.hpp:21-61). */
+enum { ISP_BAYER_RGGB = 0, ISP_BAYER_BGGR = 1, ISP_BAYER_GRBG = 2, ISP_BAYER_GBRG = 3 };
+enum { ISP_RAW_U8 = 0, ISP_RAW_U16 = 1, ISP_RAW_RAW10 = 2, ISP_RAW_RAW12 = 3 };
+enum { ISP_DEMOSAIC_BILINEAR = 0, ISP_DEMOSAIC_MALVAR = 1 };
+enum { ISP_WB_MANUAL = 0, ISP_WB_GRAY_WORLD = 1, ISP_WB_WHITE_PATCH = 2 };
+enum { ISP_TONE_SRGB = 0, ISP_TONE_GAMMA = 1, ISP_TONE_LINEAR = 2, ISP_TONE_LUT = 3 };
+enum { ISP_OUT_RGB8 = 0, ISP_OUT_RGBA8 = 1, ISP_OUT_RGB16 = 2, ISP_OUT_RGB32F = 3 };
+
+/* Layouts of the outputs (isp_params.hpp:166-198): histogram rows luma, R, G, B of
+ * 256 bins each; a 12-float statistics vector, layout version 1. */
+#define ISP_HISTOGRAM_BINS 256
+#define ISP_HISTOGRAM_CHANNELS 4
+#define ISP_STATS_SIZE 12
+#define ISP_STATS_LAYOUT_VERSION 1
+#define ISP_TONE_LUT_SIZE 4097
+
+/* AutoExposureParams (isp_params.hpp:82-93). */
+typedef struct isp_auto_exposure_c {
+  float target;
+  float damping;
+  int64_t min_exposure_ns;
+  int64_t max_exposure_ns;
+  float min_gain;
+  float max_gain;
+} isp_auto_exposure_c;
+
+/* IspParams (isp_params.hpp:95-121). The optionals carry a has_ flag; the
+ * vectors are borrowed pointers with counts, read only during the call that
+ * takes them (create copies what it keeps). */
+typedef struct isp_params_c {
+  float black_level;
+  int32_t has_channel_black_levels;
+  float channel_black_levels[4];
+  float white_level;
+  int32_t has_lens_shading;
+  int32_t lsc_width;      /* grid points across, 2..256 */
+  int32_t lsc_height;     /* grid points down, 2..256 */
+  int32_t lsc_channels;   /* 1 or 4 */
+  const float* lsc_gains; /* [height][width][channels] */
+  size_t lsc_gains_count;
+  int32_t white_balance;
+  float wb_gains[3];
+  float awb_smoothing;
+  float white_patch_percentile;
+  int32_t demosaic;
+  float ccm[9];
+  int32_t tone_curve;
+  float gamma;
+  const float* lut; /* ISP_TONE_LUT: 2..65536 entries */
+  size_t lut_size;
+  float sharpen;
+  isp_auto_exposure_c auto_exposure;
+} isp_params_c;
+
+/* RawImageView (isp_params.hpp:132-140). pitch is the row stride in bytes. */
+typedef struct isp_raw_view_c {
+  const void* data;
+  int32_t width;
+  int32_t height;
+  size_t pitch;
+  int32_t format;
+  int32_t bit_depth;
+  int32_t pattern;
+} isp_raw_view_c;
+
+/* RgbImageView (isp_params.hpp:143-147). */
+typedef struct isp_rgb_view_c {
+  void* data;
+  size_t pitch;
+  int32_t format;
+} isp_rgb_view_c;
+
+/* StatsOutput (isp_params.hpp:151-154); either pointer may be null. */
+typedef struct isp_stats_c {
+  uint32_t* histogram; /* ISP_HISTOGRAM_CHANNELS x ISP_HISTOGRAM_BINS */
+  float* stats;        /* ISP_STATS_SIZE */
+} isp_stats_c;
+
+/* FrameExposure (isp_params.hpp:157-160); 0 is unknown. */
+typedef struct isp_exposure_c {
+  int64_t exposure_ns;
+  float gain;
+} isp_exposure_c;
+
+typedef struct isp_b200_pipeline isp_b200_pipeline;
+
+/* ---- Library ---------------------------------------------------------- */
+
+/* ISP_B200_ABI_VERSION of the loaded library. No reference counterpart. */
+int isp_b200_abi_version(void);
+
+/* The calling thread's last error message ("" after success). */
+const char* isp_b200_last_error(void);
+
+/* The cudaError_t of the calling thread's last ISP_ECUDA, else 0. */
+int isp_b200_last_cuda_error(void);
+
+/* ---- Settings (isp_params.cpp) ------------------------------------------ */
+
+/* IspParams{} defaults (isp_params.hpp:95-121). */
+void isp_b200_params_default(isp_params_c* params);
+
+/* validate_params (isp_params.cpp:85-164): ISP_EINVAL naming the first unusable field. */
+int isp_b200_validate_params(const isp_params_c* params);
+
+/* validate_raw (isp_params.cpp:199-237). */
+int isp_b200_validate_raw(const isp_raw_view_c* raw, const isp_params_c* params);
+
+/* raw_row_bytes (isp_params.cpp:184-197). */
+size_t isp_b200_raw_row_bytes(int32_t format, int32_t width);
+
+/* tone_lut (isp_params.cpp:166-182): the table the pipeline interpolates.
+ * Writes min(size, capacity) entries to out (may be null) and the size to *size. */
+int isp_b200_tone_lut(const isp_params_c* params, float* out, size_t capacity, size_t* size);
+
+/* ---- One pipeline, one camera (isp_pipeline.hpp:39-74) ----------------- */
+
+/* IspPipeline(Backend::kCuda, params) (isp_pipeline.cpp:43-52, cuda_pipeline.cu:226-251):
+ * validates, builds the tone table, and keeps it, the lens shading grid, the
+ * white balance state and the scratch sums resident on the current device. */
+int isp_b200_create(const isp_params_c* params, isp_b200_pipeline** out);
+
+/* ~IspPipeline: waits for the pipeline's queued work, then frees it. Null is a no-op. */
+void isp_b200_destroy(isp_b200_pipeline* pipeline);
+
+/* IspPipeline::reset (isp_pipeline.cpp:58-63): forgets the white balance
+ * estimate after the queued frames finish. */
+int isp_b200_reset(isp_b200_pipeline* pipeline);
+
+/* IspPipeline::process with device memory (isp_pipeline.cpp:65-90,
+ * cuda_pipeline.cu:294-364): raw, out, histogram and stats are device
+ * pointers; the work is queued on `stream` (a cudaStream_t, null for the
+ * legacy default stream). Consecutive calls run on the GPU in call order, even
+ * across streams. stats and exposure may be null. */
+int isp_b200_process(isp_b200_pipeline* pipeline, const isp_raw_view_c* raw,
+                     const isp_rgb_view_c* out, const isp_stats_c* stats,
+                     const isp_exposure_c* exposure, void* stream);
+
+/* IspPipeline(Backend::kCpu)::process's contract with the GPU behind it
+ * (isp_pipeline.cpp:82-84): raw, out, histogram and stats are HOST pointers and
+ * the results are there when the call returns. The pipeline stages through its
+ * own pinned and device buffers, grown on demand. */
+int isp_b200_process_host(isp_b200_pipeline* pipeline, const isp_raw_view_c* raw,
+                          const isp_rgb_view_c* out, const isp_stats_c* stats,
+                          const isp_exposure_c* exposure);
+
+/* The white balance gains (R, G, B) and validity the next frame starts from:
+ * AwbState (isp_math.hpp:71-74). Waits for the queued frames. */
+int isp_b200_awb_state(isp_b200_pipeline* pipeline, float gains[3], int32_t* valid);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* ISP_B200_H_ */
