@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 ISP: Gpix/s on one frame shape, bit-exact path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c1]
+
+A step is one frame through the ISP. The default workload is a 3840x2160
+GRBG MIPI RAW10 frame with gray-world white balance, Malvar-He-Cutler
+demosaic, sharpening 0.5, the colour matrix, a 1024-entry sRGB table, RGB16
+output, histogram and statistics (the HBM-roofline frame shape). Frames are
+independent, so N GPUs run N replicas on their own frames (weak scaling, no
+collective on the data path); torch.distributed is used only for the barrier
+and the max over ranks of the timed region.
+
+`value` is device-resident throughput (inputs already in HBM, rotating over
+buffer sets that together exceed L2), timed with CUDA events on the
+launching stream. `e2e` is the same metric through the host-buffer C-ABI call
+(isp_b200_process_host: host->device copy of the raw frame, the kernels, and
+the device->host copy of the image, histogram and statistics, every step).
+`roofline` is the fused tile kernel's compulsory bytes over its own
+event-timed duration. `cpu_baseline` is the reference's CPU backend (built
+from its sources into oracle/_ref) on the host cores, a bounded sample.
+
+--impl reference times that CPU backend alone on the same workload and prints
+the same line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "holoscan-zozo-modules_b200"))
+
+import numpy as np  # noqa: E402
+
+from isp_b200 import abi, scene  # noqa: E402
+
+L2_BYTES = 126 * 1024 * 1024
+METRIC = "ISP Gpix/s (bit-exact vs the reference CPU backend)"
+WORKLOADS = {"c0": scene.config0, "c1": scene.config1, "c2": scene.config2}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str, workload: str):
+    """dram bytes per launch of `kernel` from its committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(float(line.split(":", 1)[1].strip()))
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi samples of the GPU's clocks and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.device)], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ---- CPU: the reference's own backend on the host cores ---------------------
+
+def cpu_pipeline_factory():
+    """The reference CPU backend (oracle/_ref) where built, else the C oracle."""
+    import oracle
+
+    if oracle.reference_available():
+        return oracle.ReferencePipeline, "reference"
+    return oracle.OraclePipeline, "port"
+
+
+def cpu_threads() -> int:
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+
+        n = min(n, max(1, int(psutil.virtual_memory().available // (400 * 1024 * 1024))))
+    except ImportError:
+        pass
+    return max(1, min(n, 64))
+
+
+def cpu_throughput(w: scene.Workload, raw: abi.RawFrame, seconds: float, threads: int):
+    """Frames per second of `threads` independent CPU pipelines for about `seconds`."""
+    make, kind = cpu_pipeline_factory()
+    pipes = [make(w.params) for _ in range(threads)]
+    for p in pipes[:1]:
+        p.process(raw, w.out_format, w.with_stats)  # warm-up: first touches of the scratch
+    counts = [0] * threads
+    stop = time.perf_counter() + seconds
+
+    def work(i):
+        p = pipes[i]
+        while time.perf_counter() < stop or counts[i] == 0:
+            p.process(raw, w.out_format, w.with_stats)
+            counts[i] += 1
+
+    t0 = time.perf_counter()
+    ts = [threading.Thread(target=work, args=(i,)) for i in range(threads)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    elapsed = time.perf_counter() - t0
+    frames = sum(counts)
+    return frames, elapsed, kind
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    w = WORKLOADS[args.workload]()
+    raw = w.raw(1)
+    threads = cpu_threads()
+    make, kind = cpu_pipeline_factory()
+    pipes = [make(w.params) for _ in range(threads)]
+    step_times = []
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ts = [threading.Thread(target=pipes[i].process, args=(raw, w.out_format, w.with_stats)) for i in range(threads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        if step >= args.warmup:
+            step_times.append(time.perf_counter() - t0)
+    total = sum(step_times)
+    value = threads * w.pixels * len(step_times) / total / 1e9
+    sample = f"{threads} threads x 1 frame of {w.width}x{w.height} per step"
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gpix/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total / len(step_times) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
+        "config": workload_config(w), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "Gpix/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(w: scene.Workload, nbuf: int = 0):
+    cfg = {"workload": w.name, "width": w.width, "height": w.height,
+           "pattern": ["RGGB", "BGGR", "GRBG", "GBRG"][w.pattern], "raw_format": ["u8", "u16", "RAW10", "RAW12"][w.fmt],
+           "bit_depth": w.bits, "output": ["RGB8", "RGBA8", "RGB16", "RGB32F"][w.out_format],
+           "white_balance": ["manual", "gray-world", "white-patch"][w.params.white_balance],
+           "demosaic": ["bilinear", "malvar"][w.params.demosaic], "sharpen": w.params.sharpen,
+           "histogram": w.with_hist, "stats": w.with_stats, "compulsory_bytes_per_frame": w.compulsory_bytes()}
+    if nbuf:
+        cfg["l2"] = f"{nbuf} rotating buffer sets, {nbuf * w.compulsory_bytes() / 1e6:.0f} MB > 126 MB L2"
+    return cfg
+
+
+# ---- GPU ---------------------------------------------------------------------
+
+def run_b200(args):
+    import torch
+
+    import isp_b200
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    w = WORKLOADS[args.workload]()
+    raw = w.raw(1 + rank)
+    out_row = w.width * abi.output_channels(w.out_format) * abi.output_channel_bytes(w.out_format)
+    nbuf = max(2, math.ceil(2 * L2_BYTES / w.compulsory_bytes()))
+    raws = [torch.from_numpy(raw.data).cuda() for _ in range(nbuf)]
+    outs = [torch.empty(w.height * out_row, dtype=torch.uint8, device="cuda") for _ in range(nbuf)]
+    hists = [torch.empty(1024, dtype=torch.int32, device="cuda") for _ in range(nbuf)]
+    stats = [torch.empty(12, dtype=torch.float32, device="cuda") for _ in range(nbuf)]
+    pipe = isp_b200.Pipeline(w.params)
+    views = []
+    for i in range(nbuf):
+        rv = abi.RawViewC(raws[i].data_ptr(), w.width, w.height, raw.pitch, w.fmt, w.bits, w.pattern)
+        ov = abi.RgbViewC(outs[i].data_ptr(), out_row, w.out_format)
+        st = abi.StatsC(hists[i].data_ptr() if w.with_hist else None, stats[i].data_ptr() if w.with_stats else None)
+        views.append((rv, ov, st))
+    exp = abi.ExposureC(10_000_000, 2.0)
+    L = isp_b200.lib()
+    stream = torch.cuda.Stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+
+    def step(i):
+        rv, ov, st = views[i % nbuf]
+        isp_b200.check(L.isp_b200_process(pipe.handle, C.byref(rv), C.byref(ov), C.byref(st), C.byref(exp), sptr))
+
+    launches_per_step = 2 if w.params.white_balance != abi.MANUAL else 1
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+        # Per-step events around the fused tile kernel (the roofline's kernel).
+        before = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        after = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        for e in before + after:
+            e.record(stream)  # creates the CUDA event behind the handle
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        clocks = Clocks(local)
+        clocks.start()
+        time.sleep(0.3)
+        barrier()
+        start.record(stream)
+        for i in range(args.steps):
+            L.isp_b200_set_kernel_events(pipe.handle, C.c_void_p(before[i].cuda_event), C.c_void_p(after[i].cuda_event))
+            step(i)
+        end.record(stream)
+        L.isp_b200_set_kernel_events(pipe.handle, None, None)
+        barrier()
+        clock_info = clocks.stop()
+    elapsed_ms = start.elapsed_time(end)
+    kernel_ms = sum(b.elapsed_time(a) for b, a in zip(before, after)) / args.steps
+    t = torch.tensor([elapsed_ms], device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_max = float(t.item())
+    value = world * args.steps * w.pixels / (elapsed_max / 1e3) / 1e9
+
+    # End to end through the host-buffer call, pinned host memory, every step.
+    e2e_steps = max(3, min(args.steps, 40))
+    host_raw = torch.from_numpy(raw.data).pin_memory().numpy()
+    host_raw_frame = abi.RawFrame(host_raw, w.width, w.height, raw.pitch, w.fmt, w.bits, w.pattern)
+    host_out = torch.empty((w.height, out_row), dtype=torch.uint8).pin_memory().numpy()
+    host_out_typed = host_out.view(abi.output_dtype(w.out_format)).reshape(w.height, w.width, abi.output_channels(w.out_format))
+    for _ in range(3):
+        pipe.process_host(host_raw_frame, w.out_format, w.with_stats, (10_000_000, 2.0), out=host_out_typed)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        pipe.process_host(host_raw_frame, w.out_format, w.with_stats, (10_000_000, 2.0), out=host_out_typed)
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps * w.pixels / float(t.item()) / 1e9
+    h2d = abi.raw_row_bytes(w.fmt, w.width) * w.height
+    d2h = w.height * out_row + (4096 if w.with_hist else 0) + (48 if w.with_stats else 0)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = cpu_threads()
+        frames, secs, kind = cpu_throughput(w, raw, args.cpu_seconds, threads)
+        cpu = {"value": frames * w.pixels / secs / 1e9, "unit": "Gpix/s", "cores": threads, "kind": kind,
+               "sample": f"{frames} frames of {w.width}x{w.height} over {secs:.1f} s on {threads} threads"}
+
+    if dist is not None:
+        dist.barrier()
+    pipe.close()
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        achieved = w.compulsory_bytes() / (kernel_ms / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gpix/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
+            "config": workload_config(w, nbuf),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profiled_traffic("isp_main_kernel", args.workload),
+                         "kernel": "isp_main_kernel", "kernel_ms": kernel_ms, "peak_kind": peak_kind},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "Gpix/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps, "api": "isp_b200_process_host"},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clock_info,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

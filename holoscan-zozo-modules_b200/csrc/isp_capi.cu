@@ -1,0 +1,474 @@
+// isp_capi.cu - the C ABI of the B200 ISP (include/isp_b200.h): one
+// pipeline per camera, its resident device state, and frame submission.
+//
+// Mirrors holoscan::isp::IspPipeline with the CUDA backend
+// (modules/isp/src/isp_pipeline.cpp:37-90, cuda_pipeline.cu:226-364): the
+// same validation and errors, frames of one pipeline ordered on the GPU by an
+// event even across streams, all work asynchronous on the caller's stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "isp_b200.h"
+#include "isp_host.hpp"
+#include "isp_kernels.cuh"
+
+namespace isp_b200 {
+
+namespace {
+
+thread_local std::string t_error;
+thread_local int t_cuda_error = 0;
+
+// The channel at quad position (y & 1) * 2 + (x & 1) per pattern (cpu_pipeline.cpp:15-20).
+constexpr int kCfa[4][4] = {
+    {kChR, kChGr, kChGb, kChB},
+    {kChB, kChGb, kChGr, kChR},
+    {kChGr, kChR, kChB, kChGb},
+    {kChGb, kChB, kChR, kChGr},
+};
+
+std::mutex g_shapes_mutex;
+std::vector<LaunchShapes> g_shapes;  // per device
+
+}  // namespace
+
+int fail(int status, const std::string& message) {
+  t_error = message;
+  t_cuda_error = 0;
+  return status;
+}
+
+int fail_cuda(cudaError_t error, const char* what) {
+  t_error = std::string(what) + ": " + cudaGetErrorString(error);
+  t_cuda_error = static_cast<int>(error);
+  return ISP_ECUDA;
+}
+
+void clear_error() {
+  t_error.clear();
+  t_cuda_error = 0;
+}
+
+namespace {
+
+// Copies on a stream of their own, waited for: the caller's streams (blocking
+// or not) neither wait for these nor are waited for (cuda_pipeline.cu:281-292).
+struct PrivateStream {
+  cudaStream_t s = nullptr;
+  cudaError_t error = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  ~PrivateStream() {
+    if (s != nullptr) cudaStreamDestroy(s);
+  }
+  cudaError_t copy(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    if (error == cudaSuccess) error = cudaMemcpyAsync(dst, src, bytes, kind, s);
+    return error;
+  }
+  cudaError_t zero(void* dst, size_t bytes) {
+    if (error == cudaSuccess) error = cudaMemsetAsync(dst, 0, bytes, s);
+    return error;
+  }
+  cudaError_t finish() {
+    if (error == cudaSuccess) error = cudaStreamSynchronize(s);
+    return error;
+  }
+};
+
+}  // namespace
+
+cudaError_t device_state_create(const isp_params_c& p, DeviceState* s) {
+  const std::vector<float> lut = tone_lut(p);
+  const int n = static_cast<int>(lut.size());
+  std::vector<float2> pairs(static_cast<size_t>(n));
+  for (int i = 0; i + 1 < n; ++i) pairs[static_cast<size_t>(i)] = make_float2(lut[i], lut[i + 1] - lut[i]);
+  pairs[static_cast<size_t>(n - 1)] = make_float2(lut[n - 1], 0.0F);
+  s->tone_size = n;
+  s->tone_last = lut[static_cast<size_t>(n - 1)];
+  PrivateStream ps;
+  cudaError_t e = ps.error;
+  if (e == cudaSuccess) e = cudaMalloc(&s->tone, pairs.size() * sizeof(float2));
+  if (e == cudaSuccess) e = ps.copy(s->tone, pairs.data(), pairs.size() * sizeof(float2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && p.has_lens_shading) {
+    e = cudaMalloc(&s->lsc, p.lsc_gains_count * sizeof(float));
+    if (e == cudaSuccess) e = ps.copy(s->lsc, p.lsc_gains, p.lsc_gains_count * sizeof(float), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&s->scratch, sizeof(Scratch));
+  if (e == cudaSuccess) e = ps.zero(s->scratch, sizeof(Scratch));
+  if (e == cudaSuccess) e = ps.finish();
+  if (e == cudaSuccess) e = device_state_reset_awb(p, s, nullptr);
+  if (e != cudaSuccess) device_state_free(s);
+  return e;
+}
+
+void device_state_free(DeviceState* s) {
+  cudaFree(s->tone);
+  cudaFree(s->lsc);
+  cudaFree(s->scratch);
+  *s = DeviceState{};
+}
+
+cudaError_t device_state_reset_awb(const isp_params_c& p, DeviceState* s, cudaStream_t stream) {
+  struct {
+    float gains[3];
+    int valid;
+  } init = {{p.wb_gains[0], p.wb_gains[1], p.wb_gains[2]}, 0};
+  static_assert(sizeof(init) == sizeof(float) * 3 + sizeof(int), "AwbState layout");
+  if (stream != nullptr) {
+    const cudaError_t e = cudaMemcpyAsync(&s->scratch->awb_gains[0], &init, sizeof(init), cudaMemcpyHostToDevice, stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(stream) : e;
+  }
+  PrivateStream ps;
+  ps.copy(&s->scratch->awb_gains[0], &init, sizeof(init), cudaMemcpyHostToDevice);
+  return ps.finish();
+}
+
+FrameDesc make_desc(const isp_params_c& p, const DeviceState& s, const isp_raw_view_c& raw,
+                    const isp_rgb_view_c& out, const isp_stats_c* stats, const isp_exposure_c* exposure) {
+  FrameDesc d{};
+  d.width = raw.width;
+  d.height = raw.height;
+  d.raw = static_cast<const uint8_t*>(raw.data);
+  d.raw_pitch = static_cast<int64_t>(raw.pitch);
+  d.raw_format = raw.format;
+  for (int k = 0; k < 4; ++k) d.cfa[k] = kCfa[raw.pattern][k];
+  const float white = white_level_of(p, raw.bit_depth);
+  for (int k = 0; k < 4; ++k) {
+    d.black[k] = p.has_channel_black_levels ? p.channel_black_levels[k] : p.black_level;
+    d.inv_range[k] = 1.0F / (white - d.black[k]);
+  }
+  d.white = static_cast<int>(std::ceil(white));
+  for (int k = 0; k < 3; ++k) d.wb[k] = p.wb_gains[k];
+  d.auto_wb = p.white_balance != ISP_WB_MANUAL;
+  if (p.has_lens_shading) {
+    d.lsc = s.lsc;
+    d.lsc_width = p.lsc_width;
+    d.lsc_height = p.lsc_height;
+    d.lsc_channels = p.lsc_channels;
+    d.lsc_sx = static_cast<float>(p.lsc_width - 1) / static_cast<float>(raw.width - 1);
+    d.lsc_sy = static_cast<float>(p.lsc_height - 1) / static_cast<float>(raw.height - 1);
+  }
+  for (int k = 0; k < 9; ++k) d.ccm[k] = p.ccm[k];
+  d.tone = s.tone;
+  d.tone_size = s.tone_size;
+  d.tone_last = s.tone_last;
+  d.sharpen = p.sharpen;
+  d.out = static_cast<uint8_t*>(out.data);
+  d.out_pitch = static_cast<int64_t>(out.pitch);
+  d.out_format = out.format;
+  d.out_vector = (reinterpret_cast<uintptr_t>(out.data) % 16U == 0U) && (out.pitch % 16U == 0U);
+  d.hist_out = stats != nullptr ? stats->histogram : nullptr;
+  d.stats_out = stats != nullptr ? stats->stats : nullptr;
+  d.scratch = s.scratch;
+  d.ae.target = p.auto_exposure.target;
+  d.ae.damping = p.auto_exposure.damping;
+  d.ae.min_exposure_ns = p.auto_exposure.min_exposure_ns;
+  d.ae.max_exposure_ns = p.auto_exposure.max_exposure_ns;
+  d.ae.min_gain = p.auto_exposure.min_gain;
+  d.ae.max_gain = p.auto_exposure.max_gain;
+  d.exposure_ns = exposure != nullptr ? exposure->exposure_ns : 0;
+  d.exposure_gain = exposure != nullptr ? exposure->gain : 0.0F;
+  d.awb_mode = p.white_balance;
+  d.awb_percentile = p.white_patch_percentile;
+  d.awb_smoothing = p.awb_smoothing;
+  return d;
+}
+
+namespace {
+
+LaunchShapes& shapes_for_current_device(cudaError_t* error) {
+  int device = 0;
+  *error = cudaGetDevice(&device);
+  std::lock_guard<std::mutex> lock(g_shapes_mutex);
+  if (g_shapes.size() <= static_cast<size_t>(device)) g_shapes.resize(static_cast<size_t>(device) + 1);
+  LaunchShapes& s = g_shapes[static_cast<size_t>(device)];
+  if (s.sm_count == 0 && *error == cudaSuccess) {
+    *error = cudaDeviceGetAttribute(&s.sm_count, cudaDevAttrMultiProcessorCount, device);
+  }
+  return s;
+}
+
+}  // namespace
+
+cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes& shapes, cudaStream_t stream,
+                         cudaEvent_t before_main, cudaEvent_t after_main) {
+  const int threads = kernel_threads();
+  if (d.auto_wb) {
+    const bool white_patch = p.white_balance == ISP_WB_WHITE_PATCH;
+    const void* k = awb_kernel(white_patch);
+    int& bpsm = shapes.awb_blocks_per_sm[white_patch ? 1 : 0];
+    if (bpsm == 0) {
+      const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k, threads, 0);
+      if (e != cudaSuccess) return e;
+      bpsm = std::max(bpsm, 1);
+    }
+    const int64_t quads = static_cast<int64_t>(d.width / 2) * (d.height / 2);
+    const int64_t wanted = (quads + threads - 1) / threads;
+    const int blocks = static_cast<int>(std::clamp<int64_t>(wanted, 1, static_cast<int64_t>(shapes.sm_count) * bpsm));
+    FrameDesc desc = d;
+    const float* lsc = d.lsc;
+    void* args[] = {&desc, &lsc};
+    const cudaError_t e = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, 0, stream);
+    if (e != cudaSuccess) return e;
+  }
+  const bool malvar = p.demosaic == ISP_DEMOSAIC_MALVAR;
+  const bool sharpen = p.sharpen > 0.0F;
+  const void* k = main_kernel(malvar, sharpen, d.out_format);
+  int& bpsm = shapes.main_blocks_per_sm[malvar][sharpen][d.out_format];
+  size_t& smem = shapes.main_smem[malvar][sharpen][d.out_format];
+  const size_t need = main_kernel_smem(sharpen, d.tone_size);
+  if (bpsm == 0 || smem < need) {
+    // Sized for the largest shared footprint this instance has met.
+    smem = std::max(smem, need);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k, threads, smem);
+    if (e != cudaSuccess) return e;
+    bpsm = std::max(bpsm, 1);
+  }
+  int tiles_x = 0;
+  const int tiles = main_kernel_tiles(d.width, d.height, &tiles_x);
+  const int blocks = std::min(tiles, shapes.sm_count * bpsm);
+  FrameDesc desc = d;
+  void* args[] = {&desc, &tiles_x, const_cast<int*>(&tiles)};
+  if (before_main != nullptr) {
+    const cudaError_t e = cudaEventRecord(before_main, stream);
+    if (e != cudaSuccess) return e;
+  }
+  const cudaError_t e = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, need, stream);
+  if (e != cudaSuccess || after_main == nullptr) return e;
+  return cudaEventRecord(after_main, stream);
+}
+
+}  // namespace isp_b200
+
+using namespace isp_b200;
+
+struct isp_b200_pipeline {
+  OwnedParams params;
+  DeviceState state;
+  int device = 0;
+  cudaEvent_t done = nullptr;
+  bool queued = false;
+  // Staging for isp_b200_process_host, grown on demand.
+  cudaStream_t host_stream = nullptr;
+  void* d_raw = nullptr;
+  size_t d_raw_cap = 0;
+  void* d_out = nullptr;
+  size_t d_out_cap = 0;
+  void* d_stats = nullptr;  // histogram then statistics
+  // Profiling events around the fused tile kernel (isp_b200_set_kernel_events).
+  cudaEvent_t before_main = nullptr;
+  cudaEvent_t after_main = nullptr;
+};
+
+extern "C" {
+
+int isp_b200_abi_version(void) { return ISP_B200_ABI_VERSION; }
+
+const char* isp_b200_last_error(void) { return t_error.c_str(); }
+
+int isp_b200_last_cuda_error(void) { return t_cuda_error; }
+
+void isp_b200_params_default(isp_params_c* params) {
+  if (params != nullptr) params_default(params);
+}
+
+int isp_b200_validate_params(const isp_params_c* params) {
+  if (params == nullptr) return fail(ISP_EINVAL, "params is null");
+  if (const char* why = validate_params(*params)) return fail(ISP_EINVAL, why);
+  clear_error();
+  return ISP_OK;
+}
+
+int isp_b200_validate_raw(const isp_raw_view_c* raw, const isp_params_c* params) {
+  if (raw == nullptr || params == nullptr) return fail(ISP_EINVAL, "raw view or params is null");
+  const std::string why = validate_raw(*raw, *params);
+  if (!why.empty()) return fail(ISP_EINVAL, why);
+  clear_error();
+  return ISP_OK;
+}
+
+size_t isp_b200_raw_row_bytes(int32_t format, int32_t width) { return raw_row_bytes(format, width); }
+
+int isp_b200_tone_lut(const isp_params_c* params, float* out, size_t capacity, size_t* size) {
+  if (params == nullptr) return fail(ISP_EINVAL, "params is null");
+  if (const char* why = validate_params(*params)) return fail(ISP_EINVAL, why);
+  const std::vector<float> lut = tone_lut(*params);
+  if (out != nullptr) std::memcpy(out, lut.data(), std::min(capacity, lut.size()) * sizeof(float));
+  if (size != nullptr) *size = lut.size();
+  clear_error();
+  return ISP_OK;
+}
+
+int isp_b200_create(const isp_params_c* params, isp_b200_pipeline** out) {
+  if (out == nullptr) return fail(ISP_EINVAL, "out is null");
+  *out = nullptr;
+  if (params == nullptr) return fail(ISP_EINVAL, "params is null");
+  if (const char* why = validate_params(*params)) return fail(ISP_EINVAL, why);
+  auto* pl = new isp_b200_pipeline;
+  pl->params.assign(*params);
+  cudaError_t e = cudaGetDevice(&pl->device);
+  if (e == cudaSuccess) e = device_state_create(pl->params.c, &pl->state);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pl->done, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    device_state_free(&pl->state);
+    delete pl;
+    return fail_cuda(e, "IspPipeline (cuda)");
+  }
+  *out = pl;
+  clear_error();
+  return ISP_OK;
+}
+
+void isp_b200_destroy(isp_b200_pipeline* pl) {
+  if (pl == nullptr) return;
+  if (pl->queued) cudaEventSynchronize(pl->done);
+  if (pl->host_stream != nullptr) cudaStreamSynchronize(pl->host_stream);
+  device_state_free(&pl->state);
+  cudaFree(pl->d_raw);
+  cudaFree(pl->d_out);
+  cudaFree(pl->d_stats);
+  if (pl->host_stream != nullptr) cudaStreamDestroy(pl->host_stream);
+  if (pl->done != nullptr) cudaEventDestroy(pl->done);
+  delete pl;
+}
+
+int isp_b200_reset(isp_b200_pipeline* pl) {
+  if (pl == nullptr) return fail(ISP_EINVAL, "pipeline is null");
+  if (pl->queued) {
+    const cudaError_t e = cudaEventSynchronize(pl->done);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaEventSynchronize");
+  }
+  const cudaError_t e = device_state_reset_awb(pl->params.c, &pl->state, nullptr);
+  if (e != cudaSuccess) return fail_cuda(e, "reset");
+  clear_error();
+  return ISP_OK;
+}
+
+int isp_b200_awb_state(isp_b200_pipeline* pl, float gains[3], int32_t* valid) {
+  if (pl == nullptr) return fail(ISP_EINVAL, "pipeline is null");
+  if (pl->queued) {
+    const cudaError_t e = cudaEventSynchronize(pl->done);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaEventSynchronize");
+  }
+  struct {
+    float g[3];
+    int v;
+  } st{};
+  PrivateStream ps;
+  ps.copy(&st, &pl->state.scratch->awb_gains[0], sizeof(st), cudaMemcpyDeviceToHost);
+  const cudaError_t e = ps.finish();
+  if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyAsync");
+  if (gains != nullptr) {
+    for (int k = 0; k < 3; ++k) gains[k] = st.g[k];
+  }
+  if (valid != nullptr) *valid = st.v;
+  clear_error();
+  return ISP_OK;
+}
+
+int isp_b200_process(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp_rgb_view_c* out,
+                     const isp_stats_c* stats, const isp_exposure_c* exposure, void* stream_ptr) {
+  if (pl == nullptr || raw == nullptr || out == nullptr) return fail(ISP_EINVAL, "pipeline, raw or out is null");
+  std::string why = validate_raw(*raw, pl->params.c);
+  if (why.empty()) why = validate_out(*raw, *out);
+  if (!why.empty()) return fail(ISP_EINVAL, why);
+  auto stream = static_cast<cudaStream_t>(stream_ptr);
+  cudaError_t error = cudaSuccess;
+  LaunchShapes& shapes = shapes_for_current_device(&error);
+  if (error != cudaSuccess) return fail_cuda(error, "cudaGetDevice");
+  const FrameDesc d = make_desc(pl->params.c, pl->state, *raw, *out, stats, exposure);
+  // Clear an error an earlier, unrelated call left (cuda_pipeline.cu:301-303).
+  static_cast<void>(cudaGetLastError());
+  // Frames share the scratch and white balance state: on another stream,
+  // the GPU waits for the previous frame first (cuda_pipeline.cu:304-310).
+  if (pl->queued) {
+    error = cudaStreamWaitEvent(stream, pl->done, 0);
+    if (error != cudaSuccess) return fail_cuda(error, "cudaStreamWaitEvent");
+  }
+  error = launch_frame(d, pl->params.c, shapes, stream, pl->before_main, pl->after_main);
+  if (error == cudaSuccess) error = cudaGetLastError();
+  if (error != cudaSuccess) return fail_cuda(error, "IspPipeline (cuda)");
+  error = cudaEventRecord(pl->done, stream);
+  if (error != cudaSuccess) return fail_cuda(error, "cudaEventRecord");
+  pl->queued = true;
+  clear_error();
+  return ISP_OK;
+}
+
+int isp_b200_set_kernel_events(isp_b200_pipeline* pl, void* before, void* after) {
+  if (pl == nullptr) return fail(ISP_EINVAL, "pipeline is null");
+  pl->before_main = static_cast<cudaEvent_t>(before);
+  pl->after_main = static_cast<cudaEvent_t>(after);
+  clear_error();
+  return ISP_OK;
+}
+
+int isp_b200_process_host(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp_rgb_view_c* out,
+                          const isp_stats_c* stats, const isp_exposure_c* exposure) {
+  if (pl == nullptr || raw == nullptr || out == nullptr) return fail(ISP_EINVAL, "pipeline, raw or out is null");
+  std::string why = validate_raw(*raw, pl->params.c);
+  if (why.empty()) why = validate_out(*raw, *out);
+  if (!why.empty()) return fail(ISP_EINVAL, why);
+  cudaError_t e = cudaSuccess;
+  if (pl->host_stream == nullptr) {
+    e = cudaStreamCreateWithFlags(&pl->host_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaStreamCreate");
+  }
+  // Device copies: raw rows packed to a 16-byte pitch, output rows packed.
+  const size_t row = raw_row_bytes(raw->format, raw->width);
+  const size_t raw_pitch = (row + 15U) & ~size_t{15};
+  const size_t raw_bytes = raw_pitch * static_cast<size_t>(raw->height);
+  const size_t cb = out->format == ISP_OUT_RGB16 ? 2U : out->format == ISP_OUT_RGB32F ? 4U : 1U;
+  const size_t out_row = static_cast<size_t>(raw->width) * (out->format == ISP_OUT_RGBA8 ? 4U : 3U) * cb;
+  const size_t out_bytes = out_row * static_cast<size_t>(raw->height);
+  const auto grow = [&](void** buffer, size_t* cap, size_t bytes) -> cudaError_t {
+    if (*cap >= bytes) return cudaSuccess;
+    cudaStreamSynchronize(pl->host_stream);
+    cudaFree(*buffer);
+    *buffer = nullptr;
+    *cap = 0;
+    const cudaError_t err = cudaMalloc(buffer, bytes);
+    if (err == cudaSuccess) *cap = bytes;
+    return err;
+  };
+  e = grow(&pl->d_raw, &pl->d_raw_cap, raw_bytes);
+  if (e == cudaSuccess) e = grow(&pl->d_out, &pl->d_out_cap, out_bytes);
+  if (e == cudaSuccess && pl->d_stats == nullptr) {
+    e = cudaMalloc(&pl->d_stats, (ISP_HISTOGRAM_CHANNELS * ISP_HISTOGRAM_BINS + ISP_STATS_SIZE) * 4U);
+  }
+  if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc");
+  cudaStream_t s = pl->host_stream;
+  e = cudaMemcpy2DAsync(pl->d_raw, raw_pitch, raw->data, raw->pitch, row, static_cast<size_t>(raw->height),
+                        cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy2DAsync");
+  isp_raw_view_c draw = *raw;
+  draw.data = pl->d_raw;
+  draw.pitch = raw_pitch;
+  const isp_rgb_view_c dout{pl->d_out, out_row, out->format};
+  auto* d_hist = static_cast<uint32_t*>(pl->d_stats);
+  float* d_st = reinterpret_cast<float*>(d_hist + ISP_HISTOGRAM_CHANNELS * ISP_HISTOGRAM_BINS);
+  const isp_stats_c dstats{stats != nullptr && stats->histogram != nullptr ? d_hist : nullptr,
+                           stats != nullptr && stats->stats != nullptr ? d_st : nullptr};
+  const int status = isp_b200_process(pl, &draw, &dout, &dstats, exposure, s);
+  if (status != ISP_OK) return status;
+  e = cudaMemcpy2DAsync(out->data, out->pitch, pl->d_out, out_row, out_row, static_cast<size_t>(raw->height),
+                        cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && dstats.histogram != nullptr) {
+    e = cudaMemcpyAsync(stats->histogram, d_hist, ISP_HISTOGRAM_CHANNELS * ISP_HISTOGRAM_BINS * 4U,
+                        cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess && dstats.stats != nullptr) {
+    e = cudaMemcpyAsync(stats->stats, d_st, ISP_STATS_SIZE * 4U, cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail_cuda(e, "IspPipeline (cuda) host staging");
+  clear_error();
+  return ISP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,80 @@
+// isp_host.hpp - host-side pieces shared by the C ABI's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "isp_b200.h"
+#include "isp_types.cuh"
+
+namespace isp_b200 {
+
+void params_default(isp_params_c* p);
+// nullptr when valid, else the message of the first unusable field.
+const char* validate_params(const isp_params_c& p);
+size_t raw_row_bytes(int32_t format, int32_t width);
+float white_level_of(const isp_params_c& p, int bit_depth);
+// Empty when usable, else the message.
+std::string validate_raw(const isp_raw_view_c& raw, const isp_params_c& p);
+std::string validate_out(const isp_raw_view_c& raw, const isp_rgb_view_c& out);
+std::vector<float> tone_lut(const isp_params_c& p);
+
+// Thread-local error reporting behind isp_b200_last_error().
+int fail(int status, const std::string& message);
+int fail_cuda(cudaError_t error, const char* what);
+void clear_error();
+
+// A deep copy of isp_params_c: its borrowed arrays owned.
+struct OwnedParams {
+  isp_params_c c{};
+  std::vector<float> lsc;
+  std::vector<float> lut;
+  void assign(const isp_params_c& p) {
+    c = p;
+    lsc.assign(p.has_lens_shading && p.lsc_gains ? p.lsc_gains : nullptr,
+               p.has_lens_shading && p.lsc_gains ? p.lsc_gains + p.lsc_gains_count : nullptr);
+    lut.assign(p.lut ? p.lut : nullptr, p.lut ? p.lut + p.lut_size : nullptr);
+    c.lsc_gains = lsc.empty() ? nullptr : lsc.data();
+    c.lut = lut.empty() ? nullptr : lut.data();
+  }
+};
+
+// The per-camera resident state on the device: the tone table as
+// (value, next - value) pairs, the lens shading grid, and the scratch
+// accumulators with the white balance state.
+struct DeviceState {
+  float2* tone = nullptr;
+  int tone_size = 0;
+  float tone_last = 0.0F;
+  float* lsc = nullptr;
+  Scratch* scratch = nullptr;
+};
+
+// Builds `state` on the current device from validated params.
+cudaError_t device_state_create(const isp_params_c& p, DeviceState* state);
+void device_state_free(DeviceState* state);
+// The initial white balance state (cpu_pipeline.cpp:90-95) written on `stream`.
+cudaError_t device_state_reset_awb(const isp_params_c& p, DeviceState* state, cudaStream_t stream);
+
+// The FrameDesc of a frame (make_frame_params, cpu_pipeline.cpp:50-88).
+FrameDesc make_desc(const isp_params_c& p, const DeviceState& state, const isp_raw_view_c& raw,
+                    const isp_rgb_view_c& out, const isp_stats_c* stats, const isp_exposure_c* exposure);
+
+// Launch shapes, per device, cached.
+struct LaunchShapes {
+  int sm_count = 0;
+  int main_blocks_per_sm[2][2][4] = {};  // [malvar][sharpen][out]
+  size_t main_smem[2][2][4] = {};
+  int awb_blocks_per_sm[2] = {};
+};
+
+// Queues one frame's kernels on `stream` (no host synchronisation).
+// before_main / after_main (may be null) are recorded around the fused tile kernel.
+cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes& shapes, cudaStream_t stream,
+                         cudaEvent_t before_main = nullptr, cudaEvent_t after_main = nullptr);
+
+}  // namespace isp_b200

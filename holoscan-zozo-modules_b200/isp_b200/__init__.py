@@ -1,0 +1,190 @@
+"""Python binding of libisp_b200.so, the B200 ISP's C ABI (include/isp_b200.h).
+
+`Pipeline` is holoscan::isp::IspPipeline with the CUDA backend
+(modules/isp/include/holoscan/isp/isp_pipeline.hpp:39-74): create from
+IspParams, `process` frames held in device memory on a CUDA stream,
+`process_host` frames held in host memory (the CPU backend's call shape),
+`reset` the white balance estimate. Errors raise as the reference's façade
+throws: ValueError for std::invalid_argument, RuntimeError for CUDA failures.
+
+The library is the product's only compute path: if it is missing or fails to
+load, every call raises; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import abi
+from .abi import IspParams, RawFrame  # noqa: F401  (re-exported)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libisp_b200.so")
+
+_lib = None
+
+
+class IspError(RuntimeError):
+    """A failed call of the C ABI; `status` is its isp_status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class IspTimeout(IspError, TimeoutError):
+    pass
+
+
+class IspBusy(IspError):
+    pass
+
+
+def lib() -> C.CDLL:
+    """The loaded C-ABI library; raises if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is not built: run holoscan-zozo-modules_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        L.isp_b200_abi_version.restype = C.c_int
+        L.isp_b200_last_error.restype = C.c_char_p
+        L.isp_b200_last_cuda_error.restype = C.c_int
+        L.isp_b200_params_default.argtypes = [P(abi.ParamsC)]
+        L.isp_b200_validate_params.argtypes = [P(abi.ParamsC)]
+        L.isp_b200_validate_raw.argtypes = [P(abi.RawViewC), P(abi.ParamsC)]
+        L.isp_b200_raw_row_bytes.restype = C.c_size_t
+        L.isp_b200_raw_row_bytes.argtypes = [C.c_int32, C.c_int32]
+        L.isp_b200_tone_lut.argtypes = [P(abi.ParamsC), C.c_void_p, C.c_size_t, P(C.c_size_t)]
+        L.isp_b200_create.argtypes = [P(abi.ParamsC), P(C.c_void_p)]
+        L.isp_b200_destroy.argtypes = [C.c_void_p]
+        L.isp_b200_reset.argtypes = [C.c_void_p]
+        L.isp_b200_awb_state.argtypes = [C.c_void_p, C.c_void_p, P(C.c_int32)]
+        L.isp_b200_process.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
+                                       P(abi.ExposureC), C.c_void_p]
+        L.isp_b200_set_kernel_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.isp_b200_process_host.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
+                                            P(abi.ExposureC)]
+        if L.isp_b200_abi_version() != abi.ABI_VERSION:
+            raise RuntimeError("libisp_b200.so ABI version mismatch")
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status == abi.OK:
+        return
+    message = lib().isp_b200_last_error().decode()
+    if status == abi.EINVAL:
+        raise ValueError(message)
+    if status == abi.ETIMEOUT:
+        raise IspTimeout(status, message)
+    if status == abi.EBUSY:
+        raise IspBusy(status, message)
+    raise IspError(status, message)
+
+
+def validate_params(params: IspParams) -> None:
+    h = params.to_c()
+    check(lib().isp_b200_validate_params(h.ref()))
+
+
+def validate_raw(raw: abi.RawViewC, params: IspParams) -> None:
+    h = params.to_c()
+    check(lib().isp_b200_validate_raw(C.byref(raw), h.ref()))
+
+
+def raw_row_bytes(fmt: int, width: int) -> int:
+    return int(lib().isp_b200_raw_row_bytes(fmt, width))
+
+
+def tone_lut(params: IspParams) -> np.ndarray:
+    h = params.to_c()
+    n = C.c_size_t()
+    check(lib().isp_b200_tone_lut(h.ref(), None, 0, C.byref(n)))
+    out = np.zeros(n.value, np.float32)
+    check(lib().isp_b200_tone_lut(h.ref(), out.ctypes.data, out.size, C.byref(n)))
+    return out
+
+
+class Result:
+    """One frame's outputs in host memory."""
+
+    def __init__(self, image: np.ndarray, histogram: Optional[np.ndarray], stats: Optional[np.ndarray]):
+        self.image = image
+        self.histogram = histogram
+        self.stats = stats
+
+
+class Pipeline:
+    """IspPipeline(Backend::kCuda, params) on the current CUDA device."""
+
+    def __init__(self, params: IspParams):
+        self.params = params
+        self._holder = params.to_c()
+        handle = C.c_void_p()
+        check(lib().isp_b200_create(self._holder.ref(), C.byref(handle)))
+        self.handle = handle
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().isp_b200_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def reset(self) -> None:
+        check(lib().isp_b200_reset(self.handle))
+
+    def awb(self) -> Tuple[np.ndarray, int]:
+        gains = (C.c_float * 3)()
+        valid = C.c_int32()
+        check(lib().isp_b200_awb_state(self.handle, gains, C.byref(valid)))
+        return np.array(list(gains), np.float32), int(valid.value)
+
+    def set_kernel_events(self, before: int = 0, after: int = 0) -> None:
+        """Events (cudaEvent_t handles) recorded around the fused tile kernel of every later frame."""
+        check(lib().isp_b200_set_kernel_events(self.handle, before or None, after or None))
+
+    def process(self, raw: abi.RawViewC, out: abi.RgbViewC, histogram_ptr: int = 0, stats_ptr: int = 0,
+                exposure: Tuple[int, float] = (0, 0.0), stream: int = 0) -> None:
+        """Queues one frame whose buffers are device pointers, on `stream` (a cudaStream_t)."""
+        st = abi.StatsC(histogram_ptr or None, stats_ptr or None)
+        exp = abi.ExposureC(exposure[0], exposure[1])
+        check(lib().isp_b200_process(self.handle, C.byref(raw), C.byref(out), C.byref(st), C.byref(exp),
+                                     stream or None))
+
+    def process_host(self, raw: RawFrame, fmt: int, with_stats: bool = True,
+                     exposure: Tuple[int, float] = (0, 0.0), out: Optional[np.ndarray] = None) -> Result:
+        """One frame from host memory to host memory; returns when the outputs are there."""
+        ch = abi.output_channels(fmt)
+        image = out if out is not None else np.empty((raw.height, raw.width, ch), abi.output_dtype(fmt))
+        hist = np.zeros((abi.HISTOGRAM_CHANNELS, abi.HISTOGRAM_BINS), np.uint32) if with_stats else None
+        stats = np.zeros(abi.STATS_SIZE, np.float32) if with_stats else None
+        view = raw.view()
+        rgb = abi.RgbViewC(image.ctypes.data, image.strides[0], fmt)
+        st = abi.StatsC(hist.ctypes.data if hist is not None else None,
+                        stats.ctypes.data if stats is not None else None)
+        exp = abi.ExposureC(exposure[0], exposure[1])
+        check(lib().isp_b200_process_host(self.handle, C.byref(view), C.byref(rgb), C.byref(st), C.byref(exp)))
+        return Result(image, hist, stats)
+
+
+def params_default() -> abi.ParamsC:
+    c = abi.ParamsC()
+    lib().isp_b200_params_default(C.byref(c))
+    return c

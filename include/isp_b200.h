@@ -21,6 +21,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define ISP_B200_API __attribute__((visibility("default")))
+#else
+#define ISP_B200_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -127,52 +133,52 @@ typedef struct isp_b200_pipeline isp_b200_pipeline;
 /* ---- Library ---------------------------------------------------------- */
 
 /* ISP_B200_ABI_VERSION of the loaded library. No reference counterpart. */
-int isp_b200_abi_version(void);
+ISP_B200_API int isp_b200_abi_version(void);
 
 /* The calling thread's last error message ("" after success). */
-const char* isp_b200_last_error(void);
+ISP_B200_API const char* isp_b200_last_error(void);
 
 /* The cudaError_t of the calling thread's last ISP_ECUDA, else 0. */
-int isp_b200_last_cuda_error(void);
+ISP_B200_API int isp_b200_last_cuda_error(void);
 
 /* ---- Settings (isp_params.cpp) ------------------------------------------ */
 
 /* IspParams{} defaults (isp_params.hpp:95-121). */
-void isp_b200_params_default(isp_params_c* params);
+ISP_B200_API void isp_b200_params_default(isp_params_c* params);
 
 /* validate_params (isp_params.cpp:85-164): ISP_EINVAL naming the first unusable field. */
-int isp_b200_validate_params(const isp_params_c* params);
+ISP_B200_API int isp_b200_validate_params(const isp_params_c* params);
 
 /* validate_raw (isp_params.cpp:199-237). */
-int isp_b200_validate_raw(const isp_raw_view_c* raw, const isp_params_c* params);
+ISP_B200_API int isp_b200_validate_raw(const isp_raw_view_c* raw, const isp_params_c* params);
 
 /* raw_row_bytes (isp_params.cpp:184-197). */
-size_t isp_b200_raw_row_bytes(int32_t format, int32_t width);
+ISP_B200_API size_t isp_b200_raw_row_bytes(int32_t format, int32_t width);
 
 /* tone_lut (isp_params.cpp:166-182): the table the pipeline interpolates.
  * Writes min(size, capacity) entries to out (may be null) and the size to *size. */
-int isp_b200_tone_lut(const isp_params_c* params, float* out, size_t capacity, size_t* size);
+ISP_B200_API int isp_b200_tone_lut(const isp_params_c* params, float* out, size_t capacity, size_t* size);
 
 /* ---- One pipeline, one camera (isp_pipeline.hpp:39-74) ----------------- */
 
 /* IspPipeline(Backend::kCuda, params) (isp_pipeline.cpp:43-52, cuda_pipeline.cu:226-251):
  * validates, builds the tone table, and keeps it, the lens shading grid, the
  * white balance state and the scratch sums resident on the current device. */
-int isp_b200_create(const isp_params_c* params, isp_b200_pipeline** out);
+ISP_B200_API int isp_b200_create(const isp_params_c* params, isp_b200_pipeline** out);
 
 /* ~IspPipeline: waits for the pipeline's queued work, then frees it. Null is a no-op. */
-void isp_b200_destroy(isp_b200_pipeline* pipeline);
+ISP_B200_API void isp_b200_destroy(isp_b200_pipeline* pipeline);
 
 /* IspPipeline::reset (isp_pipeline.cpp:58-63): forgets the white balance
  * estimate after the queued frames finish. */
-int isp_b200_reset(isp_b200_pipeline* pipeline);
+ISP_B200_API int isp_b200_reset(isp_b200_pipeline* pipeline);
 
 /* IspPipeline::process with device memory (isp_pipeline.cpp:65-90,
  * cuda_pipeline.cu:294-364): raw, out, histogram and stats are device
  * pointers; the work is queued on `stream` (a cudaStream_t, null for the
  * legacy default stream). Consecutive calls run on the GPU in call order, even
  * across streams. stats and exposure may be null. */
-int isp_b200_process(isp_b200_pipeline* pipeline, const isp_raw_view_c* raw,
+ISP_B200_API int isp_b200_process(isp_b200_pipeline* pipeline, const isp_raw_view_c* raw,
                      const isp_rgb_view_c* out, const isp_stats_c* stats,
                      const isp_exposure_c* exposure, void* stream);
 
@@ -180,13 +186,18 @@ int isp_b200_process(isp_b200_pipeline* pipeline, const isp_raw_view_c* raw,
  * (isp_pipeline.cpp:82-84): raw, out, histogram and stats are HOST pointers and
  * the results are there when the call returns. The pipeline stages through its
  * own pinned and device buffers, grown on demand. */
-int isp_b200_process_host(isp_b200_pipeline* pipeline, const isp_raw_view_c* raw,
+ISP_B200_API int isp_b200_process_host(isp_b200_pipeline* pipeline, const isp_raw_view_c* raw,
                           const isp_rgb_view_c* out, const isp_stats_c* stats,
                           const isp_exposure_c* exposure);
 
 /* The white balance gains (R, G, B) and validity the next frame starts from:
  * AwbState (isp_math.hpp:71-74). Waits for the queued frames. */
-int isp_b200_awb_state(isp_b200_pipeline* pipeline, float gains[3], int32_t* valid);
+ISP_B200_API int isp_b200_awb_state(isp_b200_pipeline* pipeline, float gains[3], int32_t* valid);
+
+/* Profiling hook, no reference counterpart: events (cudaEvent_t, may be null)
+ * that every following process call records on its stream right before and
+ * right after the fused tile kernel, so a caller can time that kernel alone. */
+ISP_B200_API int isp_b200_set_kernel_events(isp_b200_pipeline* pipeline, void* before, void* after);
 
 #ifdef __cplusplus
 } /* extern "C" */
