@@ -5,6 +5,8 @@
 // (modules/isp/src/isp_pipeline.cpp:37-90, cuda_pipeline.cu:226-364): the
 // same validation and errors, frames of one pipeline ordered on the GPU by an
 // event even across streams, all work asynchronous on the caller's stream.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -135,6 +137,7 @@ FrameDesc make_desc(const isp_params_c& p, const DeviceState& s, const isp_raw_v
   d.raw = static_cast<const uint8_t*>(raw.data);
   d.raw_pitch = static_cast<int64_t>(raw.pitch);
   d.raw_format = raw.format;
+  d.pattern = raw.pattern;
   for (int k = 0; k < 4; ++k) d.cfa[k] = kCfa[raw.pattern][k];
   const float white = white_level_of(p, raw.bit_depth);
   for (int k = 0; k < 4; ++k) {
@@ -194,33 +197,82 @@ LaunchShapes& shapes_for_current_device(cudaError_t* error) {
 
 }  // namespace
 
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      f = nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+}  // namespace
+
+bool encode_raw_map(const FrameDesc& d, int box_row_bytes, int box_rows, CUtensorMap* map) {
+  std::memset(map, 0, sizeof(*map));
+  const auto base = reinterpret_cast<uintptr_t>(d.raw);
+  if (base % 16U != 0U || d.raw_pitch % 16 != 0 || d.raw_pitch >= (int64_t{1} << 40)) return false;
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (encode == nullptr) return false;
+  const bool u16 = d.raw_format == kRawU16;
+  const cuuint64_t dims[2] = {u16 ? static_cast<cuuint64_t>(d.width) : raw_row_bytes(d.raw_format, d.width),
+                              static_cast<cuuint64_t>(d.height)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(d.raw_pitch)};
+  const cuuint32_t box[2] = {static_cast<cuuint32_t>(u16 ? box_row_bytes / 2 : box_row_bytes),
+                             static_cast<cuuint32_t>(box_rows)};
+  const cuuint32_t elem[2] = {1, 1};
+  const CUresult r = encode(map, u16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
+                            const_cast<uint8_t*>(d.raw), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    std::memset(map, 0, sizeof(*map));
+    return false;
+  }
+  return true;
+}
+
 cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes& shapes, cudaStream_t stream,
                          cudaEvent_t before_main, cudaEvent_t after_main) {
   const int threads = kernel_threads();
+  const int pattern = d.pattern;
   if (d.auto_wb) {
     const bool white_patch = p.white_balance == ISP_WB_WHITE_PATCH;
-    const void* k = awb_kernel(white_patch);
-    int& bpsm = shapes.awb_blocks_per_sm[white_patch ? 1 : 0];
+    const void* k = awb_kernel(white_patch, pattern);
+    int& bpsm = shapes.awb_blocks_per_sm[white_patch ? 1 : 0][pattern];
+    const size_t smem = awb_kernel_smem();
     if (bpsm == 0) {
-      const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k, threads, 0);
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k, threads, smem);
       if (e != cudaSuccess) return e;
       bpsm = std::max(bpsm, 1);
     }
-    const int64_t quads = static_cast<int64_t>(d.width / 2) * (d.height / 2);
-    const int64_t wanted = (quads + threads - 1) / threads;
-    const int blocks = static_cast<int>(std::clamp<int64_t>(wanted, 1, static_cast<int64_t>(shapes.sm_count) * bpsm));
+    alignas(64) CUtensorMap map;
+    int use_tma = encode_raw_map(d, awb_box_row_bytes(d.raw_format), 64, &map) ? 1 : 0;
+    int tiles_x = 0;
+    int tiles = awb_kernel_tiles(d.width, d.height, &tiles_x);
+    const int blocks = std::max(1, std::min(tiles, shapes.sm_count * bpsm));
     FrameDesc desc = d;
-    const float* lsc = d.lsc;
-    void* args[] = {&desc, &lsc};
-    const cudaError_t e = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, 0, stream);
+    void* args[] = {&map, &desc, &tiles_x, &tiles, &use_tma};
+    const cudaError_t e = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, smem, stream);
     if (e != cudaSuccess) return e;
   }
   const bool malvar = p.demosaic == ISP_DEMOSAIC_MALVAR;
   const bool sharpen = p.sharpen > 0.0F;
-  const void* k = main_kernel(malvar, sharpen, d.out_format);
-  int& bpsm = shapes.main_blocks_per_sm[malvar][sharpen][d.out_format];
-  size_t& smem = shapes.main_smem[malvar][sharpen][d.out_format];
-  const size_t need = main_kernel_smem(sharpen, d.tone_size);
+  const void* k = main_kernel(malvar, sharpen, d.out_format, pattern);
+  // The tone table goes to shared memory when that still lets two CTAs share an SM.
+  const size_t without_lut = main_kernel_smem(sharpen, d.raw_format, 0);
+  const size_t with_lut = main_kernel_smem(sharpen, d.raw_format, d.tone_size);
+  int lut_in_smem = d.tone_size <= kLutSmemEntries && with_lut <= kSmemPerTwoCtas ? 1 : 0;
+  const size_t need = lut_in_smem ? with_lut : without_lut;
+  int& bpsm = shapes.main_blocks_per_sm[malvar][sharpen][d.out_format][pattern];
+  size_t& smem = shapes.main_smem[malvar][sharpen][d.out_format][pattern];
   if (bpsm == 0 || smem < need) {
     // Sized for the largest shared footprint this instance has met.
     smem = std::max(smem, need);
@@ -229,11 +281,13 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
     if (e != cudaSuccess) return e;
     bpsm = std::max(bpsm, 1);
   }
+  alignas(64) CUtensorMap map;
+  int use_tma = encode_raw_map(d, main_box_row_bytes(d.raw_format), main_box_rows(sharpen), &map) ? 1 : 0;
   int tiles_x = 0;
-  const int tiles = main_kernel_tiles(d.width, d.height, &tiles_x);
+  int tiles = main_kernel_tiles(d.width, d.height, &tiles_x);
   const int blocks = std::min(tiles, shapes.sm_count * bpsm);
   FrameDesc desc = d;
-  void* args[] = {&desc, &tiles_x, const_cast<int*>(&tiles)};
+  void* args[] = {&map, &desc, &tiles_x, &tiles, &use_tma, &lut_in_smem};
   if (before_main != nullptr) {
     const cudaError_t e = cudaEventRecord(before_main, stream);
     if (e != cudaSuccess) return e;

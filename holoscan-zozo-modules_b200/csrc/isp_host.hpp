@@ -1,6 +1,7 @@
 // isp_host.hpp - host-side pieces shared by the C ABI's translation units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -67,10 +68,19 @@ FrameDesc make_desc(const isp_params_c& p, const DeviceState& state, const isp_r
 // Launch shapes, per device, cached.
 struct LaunchShapes {
   int sm_count = 0;
-  int main_blocks_per_sm[2][2][4] = {};  // [malvar][sharpen][out]
-  size_t main_smem[2][2][4] = {};
-  int awb_blocks_per_sm[2] = {};
+  int main_blocks_per_sm[2][2][4][4] = {};  // [malvar][sharpen][out][pattern]
+  size_t main_smem[2][2][4][4] = {};
+  int awb_blocks_per_sm[2][4] = {};  // [white patch][pattern]
 };
+
+// Dynamic shared memory that still lets two CTAs of the fused kernel share an
+// SM (228 KB per SM, 1 KB reserved per CTA, static shared memory).
+constexpr size_t kSmemPerTwoCtas = 112U * 1024U;
+
+// A 2-D TMA descriptor over the raw frame: bytes (uint16 samples for
+// ISP_RAW_U16) across, rows down, boxes of box_row_bytes x box_rows. False
+// (and a zeroed map) when the frame's base or pitch is not 16-byte aligned.
+bool encode_raw_map(const FrameDesc& d, int box_row_bytes, int box_rows, CUtensorMap* map);
 
 // Queues one frame's kernels on `stream` (no host synchronisation).
 // before_main / after_main (may be null) are recorded around the fused tile kernel.

@@ -7,19 +7,27 @@
 
 namespace isp_b200 {
 
-// Tone tables up to this many entries are copied into shared memory.
-constexpr int kLutSmemEntries = 4097;
-
-// The fused tile kernel for a demosaic method, sharpening on or off, and an
-// output format; launch with kernel_threads() threads and
+// The fused tile kernel for a demosaic method, sharpening on or off, an
+// output format and a Bayer pattern; launch with kernel_threads() threads and
 // main_kernel_smem() bytes of dynamic shared memory; arguments
-// (FrameDesc, int tiles_x, int tiles).
-const void* main_kernel(bool malvar, bool sharpen, int out_format);
-size_t main_kernel_smem(bool sharpen, int tone_size);
+// (const CUtensorMap raw_map, FrameDesc, int tiles_x, int tiles, int use_tma,
+// int lut_in_smem). The raw map's box is main_box_row_bytes() bytes (or half
+// as many uint16 samples) by main_box_rows() rows.
+const void* main_kernel(bool malvar, bool sharpen, int out_format, int pattern);
+size_t main_kernel_smem(bool sharpen, int raw_format, int lut_entries);
+int main_box_rows(bool sharpen);
+int main_box_row_bytes(int raw_format);
 int main_kernel_tiles(int width, int height, int* tiles_x);
 int kernel_threads();
 
-// The white balance statistics kernel; arguments (FrameDesc, const float* lsc).
-const void* awb_kernel(bool white_patch);
+// The white balance statistics kernel; arguments (const CUtensorMap raw_map,
+// FrameDesc, int tiles_x, int tiles, int use_tma); box awb_box_row_bytes() by 64 rows.
+const void* awb_kernel(bool white_patch, int pattern);
+size_t awb_kernel_smem();
+int awb_box_row_bytes(int raw_format);
+int awb_kernel_tiles(int width, int height, int* tiles_x);
+
+// Tone tables up to this many entries may be copied into shared memory.
+constexpr int kLutSmemEntries = 4097;
 
 }  // namespace isp_b200

@@ -36,7 +36,8 @@ struct Scratch {
   u64 saturated;
   unsigned int hist[kHistChannels * kHistBins];
   unsigned int main_done;
-  unsigned int pad[3];
+  int error;  // a bounded wait in a kernel gave up (1)
+  unsigned int pad[2];
 };
 
 struct AutoExposure {
@@ -56,6 +57,7 @@ struct FrameDesc {
   const uint8_t* raw;
   int64_t raw_pitch;
   int raw_format;
+  int pattern;
   int cfa[4];  // channel at quad position (y & 1) * 2 + (x & 1)
   float black[4];
   float inv_range[4];
