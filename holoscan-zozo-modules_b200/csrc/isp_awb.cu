@@ -1,0 +1,204 @@
+// isp_awb.cu - the white balance statistics kernel of the B200 ISP
+// (gray world and white patch): tiles of 64x64 samples arrive by TMA, the
+// complete 2x2 quads without a saturated sample are summed per colour (and
+// binned for white patch) in the block, then flushed once; the last CTA to
+// finish forms the frame's estimate (finish_white_balance, isp_math.hpp:357-384)
+// and clears the sums for the next frame.
+#include "isp_common.cuh"
+
+namespace isp_b200 {
+namespace {
+
+// ---- White balance statistics ----------------------------------------------
+
+template <bool kWhitePatch, int kPat>
+__global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant__ CUtensorMap map, FrameDesc p,
+                                                         int tiles_x, int tiles, int use_tma) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
+  constexpr int kBoxRows = 64;
+  uint8_t* box = smem;                                                  // [64][box bytes]
+  float* table = reinterpret_cast<float*>(smem + 64 * 128);             // [kLscTableRows][2][kSW]
+  int* col_mx = reinterpret_cast<int*>(table + kLscTableRows * 2 * kSW);  // [64] x 3
+  int* col_ix = col_mx + 64;
+  float* col_tx = reinterpret_cast<float*>(col_ix + 64);
+  int* row_my = reinterpret_cast<int*>(col_tx + 64);                    // [64] x 3
+  int* row_k = row_my + 64;
+  float* row_ty = reinterpret_cast<float*>(row_k + 64);
+  unsigned int* hist = reinterpret_cast<unsigned int*>(row_ty + 64);    // [3][1024]
+  __shared__ uint64_t bar;
+  __shared__ u64 red[kWarps];
+  __shared__ int minmax[2];
+  __shared__ int first;
+  __shared__ bool last;
+  Scratch* s = p.scratch;
+  const int tid = threadIdx.x;
+  const int box_bytes = p.raw_format == kRawU8 ? 64 : p.raw_format == kRawU16 ? 128 : p.raw_format == kRawRaw10 ? 80 : 96;
+  if constexpr (kWhitePatch) {
+    for (int i = tid; i < 3 * kAwbBins; i += kThreads) hist[i] = 0U;
+  }
+  if (tid == 0 && use_tma) mbar_init(&bar);
+  __syncthreads();
+  // Per quad position: channel, colour, black, 1 / range.
+  float black[4], inv[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    black[k] = p.black[cfa_of(kPat, k)];
+    inv[k] = p.inv_range[cfa_of(kPat, k)];
+  }
+  const int quads_x = p.width / 2;
+  const int quads_y = p.height / 2;
+  u64 acc[4] = {0, 0, 0, 0};
+  uint32_t phase = 0;
+  int tile = blockIdx.x;
+  auto issue = [&](int t) {
+    const int ty = t / tiles_x;
+    const int x0 = (t - ty * tiles_x) * 64;
+    const int bx = p.raw_format == kRawU8 ? x0 : p.raw_format == kRawU16 ? x0 : p.raw_format == kRawRaw10 ? 5 * (x0 >> 2) : 3 * (x0 >> 1);
+    tma_load_2d(&map, box, &bar, bx, ty * 64, static_cast<unsigned int>(kBoxRows * box_bytes));
+  };
+  if (use_tma && tid == 0 && tile < tiles) issue(tile);
+  for (; tile < tiles; tile += gridDim.x) {
+    const int ty = tile / tiles_x;
+    const int x0 = (tile - ty * tiles_x) * 64;
+    const int y0 = ty * 64;
+    const LscTile lt = build_lsc(p, kPat, x0, 64, y0, 64, false, 0, 0, col_mx, col_ix, col_tx, row_my, row_k,
+                                 row_ty, table, minmax);
+    if (use_tma && !mbar_wait(&bar, phase)) {
+      if (tid == 0) atomicExch(&s->error, 1);
+    }
+    phase ^= 1U;
+    // 2 quads (4 samples across, 2 rows) per unit; 32 row pairs x 16 units.
+    for (int unit = tid; unit < 512; unit += kThreads) {
+      const int a = unit >> 4;
+      const int u = unit & 15;
+      const int qy = (y0 >> 1) + a;
+      const int qx0 = (x0 >> 1) + 2 * u;
+      if (qy >= quads_y || qx0 >= quads_x) continue;
+      unsigned int top[4], bot[4];
+      if (use_tma) {
+        // Units of 4 samples at x0 + 4u: reuse unpack4 with its x0 - 4 origin.
+        const uint8_t* r0 = box + (2 * a) * box_bytes;
+        const uint8_t* r1 = r0 + box_bytes;
+        if (p.raw_format == kRawU8) {
+          const unsigned int w0 = *reinterpret_cast<const unsigned int*>(r0 + 4 * u);
+          const unsigned int w1 = *reinterpret_cast<const unsigned int*>(r1 + 4 * u);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            top[k] = (w0 >> (8 * k)) & 0xFFU;
+            bot[k] = (w1 >> (8 * k)) & 0xFFU;
+          }
+        } else if (p.raw_format == kRawU16) {
+          const uint2 w0 = *reinterpret_cast<const uint2*>(r0 + 8 * u);
+          const uint2 w1 = *reinterpret_cast<const uint2*>(r1 + 8 * u);
+          top[0] = w0.x & 0xFFFFU; top[1] = w0.x >> 16; top[2] = w0.y & 0xFFFFU; top[3] = w0.y >> 16;
+          bot[0] = w1.x & 0xFFFFU; bot[1] = w1.x >> 16; bot[2] = w1.y & 0xFFFFU; bot[3] = w1.y >> 16;
+        } else {
+          // unpack4 reads sample x0 - 4 + 4u' from byte 11 + 5u' (RAW10) or
+          // 10 + 6u' (RAW12) of a box starting 16 bytes before x0; this box
+          // starts at x0, so shift the row pointer back 16 bytes: unit u' = u + 1.
+          unpack4(p.raw_format, r0 - 16, u + 1, top);
+          unpack4(p.raw_format, r1 - 16, u + 1, bot);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int x = x0 + 4 * u + k;
+          top[k] = x < p.width ? static_cast<unsigned int>(load_raw(p, x, y0 + 2 * a)) : 0U;
+          bot[k] = x < p.width ? static_cast<unsigned int>(load_raw(p, x, y0 + 2 * a + 1)) : 0U;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        if (qx0 + q >= quads_x) break;
+        const unsigned int raw[4] = {top[2 * q], top[2 * q + 1], bot[2 * q], bot[2 * q + 1]};
+        const bool ok = raw[0] < static_cast<unsigned int>(p.white) && raw[1] < static_cast<unsigned int>(p.white) &&
+                        raw[2] < static_cast<unsigned int>(p.white) && raw[3] < static_cast<unsigned int>(p.white);
+        if (!ok) continue;  // white_balance_quad, isp_math.hpp:311-319
+        unsigned int fixed[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int ci = 4 * u + 2 * q + (k & 1);  // column in the tile
+          const int rj = 2 * a + (k >> 1);         // row in the tile
+          float v = fmul(fsub(magic_to_float(raw[k] | kTwo23Bits), black[k]), inv[k]);
+          v = v > 0.0F ? v : 0.0F;
+          if (lt.rows > 0) {
+            float gain;
+            if (lt.rows <= kLscTableRows) {
+              const int kk = row_k[rj];
+              const int par = p.lsc_channels == 4 ? (k >> 1) : 0;
+              const float t0 = table[(kk * 2 + par) * kSW + ci];
+              const float t1 = table[((kk + 1) * 2 + par) * kSW + ci];
+              gain = fadd(t0, fmul(fsub(t1, t0), row_ty[rj]));
+            } else {
+              gain = lens_shading_gain(p, p.lsc, x0 + ci, y0 + rj, cfa_of(kPat, k));
+            }
+            v = fmul(v, gain);
+          }
+          v = v < 4.0F ? v : 4.0F;
+          fixed[k] = magic_int(magic_trunc(fadd(fmul(v, kFixedOne), 0.5F)));
+          if constexpr (kWhitePatch) {
+            const unsigned int bin = magic_int(magic_trunc(fmul(v, static_cast<float>(kAwbBins))));
+            atomicAdd(&hist[color_of(cfa_of(kPat, k)) * kAwbBins + (bin < kAwbBins - 1 ? bin : kAwbBins - 1)], 1U);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[color_of(cfa_of(kPat, k))] += fixed[k];
+        acc[3] += 1;
+      }
+    }
+    __syncthreads();
+    if (use_tma && tid == 0) {
+      const int next = tile + gridDim.x;
+      if (next < tiles) {
+        fence_async_shared();
+        issue(next);
+      }
+    }
+  }
+  // Flush: block sums, then one atomic per sum and per non-empty bin.
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    u64 v = acc[k];
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) v += __shfl_down_sync(0xFFFFFFFFU, v, offset);
+    if ((tid & 31) == 0) red[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0) {
+      u64 total = 0;
+      for (int w = 0; w < kWarps; ++w) total += red[w];
+      if (total != 0) atomicAdd(k < 3 ? &s->awb_sum[k] : &s->awb_quads, total);
+    }
+    __syncthreads();
+  }
+  if constexpr (kWhitePatch) {
+    for (int i = tid; i < 3 * kAwbBins; i += kThreads) {
+      if (hist[i] != 0U) atomicAdd(&s->awb_hist[0][0] + i, hist[i]);
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = atomicAdd(&s->awb_done, 1U) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  awb_finish(p, s, red, &first);
+}
+
+template <bool kWhitePatch>
+const void* awb_by_pattern(int pattern) {
+  switch (pattern) {
+    case 0: return reinterpret_cast<const void*>(&isp_awb_kernel<kWhitePatch, 0>);
+    case 1: return reinterpret_cast<const void*>(&isp_awb_kernel<kWhitePatch, 1>);
+    case 2: return reinterpret_cast<const void*>(&isp_awb_kernel<kWhitePatch, 2>);
+    default: return reinterpret_cast<const void*>(&isp_awb_kernel<kWhitePatch, 3>);
+  }
+}
+
+}  // namespace
+
+const void* awb_kernel(bool white_patch, int pattern) {
+  return white_patch ? awb_by_pattern<true>(pattern) : awb_by_pattern<false>(pattern);
+}
+
+}  // namespace isp_b200

@@ -265,14 +265,14 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
   }
   const bool malvar = p.demosaic == ISP_DEMOSAIC_MALVAR;
   const bool sharpen = p.sharpen > 0.0F;
-  const void* k = main_kernel(malvar, sharpen, d.out_format, pattern);
   // The tone table goes to shared memory when that still lets two CTAs share an SM.
   const size_t without_lut = main_kernel_smem(sharpen, d.raw_format, 0);
   const size_t with_lut = main_kernel_smem(sharpen, d.raw_format, d.tone_size);
   int lut_in_smem = d.tone_size <= kLutSmemEntries && with_lut <= kSmemPerTwoCtas ? 1 : 0;
   const size_t need = lut_in_smem ? with_lut : without_lut;
-  int& bpsm = shapes.main_blocks_per_sm[malvar][sharpen][d.out_format][pattern];
-  size_t& smem = shapes.main_smem[malvar][sharpen][d.out_format][pattern];
+  const void* k = main_kernel(malvar, sharpen, pattern, lut_in_smem != 0);
+  int& bpsm = shapes.main_blocks_per_sm[malvar][sharpen][d.out_format][pattern][lut_in_smem];
+  size_t& smem = shapes.main_smem[malvar][sharpen][d.out_format][pattern][lut_in_smem];
   if (bpsm == 0 || smem < need) {
     // Sized for the largest shared footprint this instance has met.
     smem = std::max(smem, need);

@@ -10,6 +10,7 @@
 
 #include <cstdint>
 
+#include "isp_ops.cuh"
 #include "isp_types.cuh"
 
 namespace isp_b200 {
@@ -81,6 +82,12 @@ __device__ __forceinline__ float linearize(const FrameDesc& p, const float* grid
 // The Malvar-He-Cutler or bilinear estimates at the centre of a 5x5
 // neighbourhood n[dy + 2][dx + 2] (isp_math.hpp:161-215), only the two that
 // the centre's channel needs. R and B sites: green and the diagonal colour.
+// In the Malvar estimates a product by 2 or 4 is exact, so round(4c + 2 a1)
+// is one fused multiply-add whose only rounding is the sum's (the reference
+// rounds the exact products, then the sum): exact_scale_add(a1, 2, 4c). The
+// products by 5, 6 and 1.5, and by 0.5 and 0.125 (exact only above the
+// subnormal range), stay separate roundings. clamp01(x * 0.125) is the
+// saturating multiply.
 template <bool kMalvar>
 __device__ __forceinline__ void estimate_rb_site(const float (&n)[5][5], float& at_green, float& diagonal) {
   if constexpr (!kMalvar) {
@@ -91,8 +98,10 @@ __device__ __forceinline__ void estimate_rb_site(const float (&n)[5][5], float& 
     const float axial1 = n[1][2] + n[3][2] + n[2][1] + n[2][3];
     const float axial2 = n[0][2] + n[4][2] + n[2][0] + n[2][4];
     const float diagonal1 = n[1][1] + n[1][3] + n[3][1] + n[3][3];
-    at_green = clamp01((4.0F * c + 2.0F * axial1 - axial2) * 0.125F);
-    diagonal = clamp01((6.0F * c + 2.0F * diagonal1 - 1.5F * axial2) * 0.125F);
+    // clamp01((4c + 2 axial1 - axial2) * 0.125)
+    at_green = mul_sat(fsub(exact_scale_add(axial1, 2.0F, fmul(4.0F, c)), axial2), 0.125F);
+    // clamp01((6c + 2 diagonal1 - 1.5 axial2) * 0.125)
+    diagonal = mul_sat(fsub(exact_scale_add(diagonal1, 2.0F, fmul(6.0F, c)), fmul(1.5F, axial2)), 0.125F);
   }
 }
 
@@ -103,13 +112,16 @@ __device__ __forceinline__ void estimate_g_site(const float (&n)[5][5], float& a
     across = (n[2][1] + n[2][3]) * 0.5F;
     down = (n[1][2] + n[3][2]) * 0.5F;
   } else {
-    const float c = n[2][2];
+    const float c5 = fmul(5.0F, n[2][2]);
     const float diagonal1 = n[1][1] + n[1][3] + n[3][1] + n[3][3];
     const float horizontal2 = n[2][0] + n[2][4];
     const float vertical2 = n[0][2] + n[4][2];
-    across = clamp01((5.0F * c + 4.0F * (n[2][1] + n[2][3]) - horizontal2 - diagonal1 + 0.5F * vertical2) *
+    // clamp01((5c + 4 (n21 + n23) - horizontal2 - diagonal1 + 0.5 vertical2) * 0.125)
+    across = mul_sat(fadd(fsub(fsub(exact_scale_add(fadd(n[2][1], n[2][3]), 4.0F, c5), horizontal2), diagonal1),
+                          fmul(0.5F, vertical2)),
                      0.125F);
-    down = clamp01((5.0F * c + 4.0F * (n[1][2] + n[3][2]) - vertical2 - diagonal1 + 0.5F * horizontal2) *
+    down = mul_sat(fadd(fsub(fsub(exact_scale_add(fadd(n[1][2], n[3][2]), 4.0F, c5), vertical2), diagonal1),
+                        fmul(0.5F, horizontal2)),
                    0.125F);
   }
 }
@@ -138,8 +150,12 @@ __device__ __forceinline__ void demosaic(const float (&n)[5][5], int channel, fl
 // that order, corners = m00, m02, m20, m22.
 __device__ __forceinline__ float sharpen_one(float c, float m01, float m21, float m10, float m12, float m00,
                                              float m02, float m20, float m22, float amount) {
-  const float blur = (4.0F * c + 2.0F * (m01 + m21 + m10 + m12) + (m00 + m02 + m20 + m22)) * 0.0625F;
-  return clamp01(c + amount * (c - blur));
+  // (4c + 2 axial + corners) * 0.0625 with round(4c + 2 axial) one fused
+  // rounding (both products exact); clamp01(c + amount (c - blur)) saturating.
+  const float axial = fadd(fadd(fadd(m01, m21), m10), m12);
+  const float corners = fadd(fadd(fadd(m00, m02), m20), m22);
+  const float blur = fmul(fadd(exact_scale_add(axial, 2.0F, fmul(4.0F, c)), corners), 0.0625F);
+  return add_sat(c, fmul(amount, fsub(c, blur)));
 }
 
 // Colour correction (isp_math.hpp:229-233).

@@ -68,8 +68,8 @@ FrameDesc make_desc(const isp_params_c& p, const DeviceState& state, const isp_r
 // Launch shapes, per device, cached.
 struct LaunchShapes {
   int sm_count = 0;
-  int main_blocks_per_sm[2][2][4][4] = {};  // [malvar][sharpen][out][pattern]
-  size_t main_smem[2][2][4][4] = {};
+  int main_blocks_per_sm[2][2][4][4][2] = {};  // [malvar][sharpen][out][pattern][lut in smem]
+  size_t main_smem[2][2][4][4][2] = {};
   int awb_blocks_per_sm[2][4] = {};  // [white patch][pattern]
 };
 

@@ -8,12 +8,12 @@
 namespace isp_b200 {
 
 // The fused tile kernel for a demosaic method, sharpening on or off, an
-// output format and a Bayer pattern; launch with kernel_threads() threads and
+// output format, a Bayer pattern and the tone table's place (shared or global); launch with kernel_threads() threads and
 // main_kernel_smem() bytes of dynamic shared memory; arguments
 // (const CUtensorMap raw_map, FrameDesc, int tiles_x, int tiles, int use_tma,
 // int lut_in_smem). The raw map's box is main_box_row_bytes() bytes (or half
 // as many uint16 samples) by main_box_rows() rows.
-const void* main_kernel(bool malvar, bool sharpen, int out_format, int pattern);
+const void* main_kernel(bool malvar, bool sharpen, int pattern, bool lut_smem);
 size_t main_kernel_smem(bool sharpen, int raw_format, int lut_entries);
 int main_box_rows(bool sharpen);
 int main_box_row_bytes(int raw_format);

@@ -1,0 +1,10 @@
+// isp_main_bilinear.cu - instances of the fused tile kernel: bilinear demosaic, sharpening off.
+#include "isp_main.cuh"
+
+namespace isp_b200 {
+
+const void* main_kernel_bn(int layout, bool lut_smem) {
+  return main_instance<false, false>(layout, lut_smem);
+}
+
+}  // namespace isp_b200

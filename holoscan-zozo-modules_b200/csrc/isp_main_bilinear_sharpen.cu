@@ -1,0 +1,10 @@
+// isp_main_bilinear_sharpen.cu - instances of the fused tile kernel: bilinear demosaic, sharpening on.
+#include "isp_main.cuh"
+
+namespace isp_b200 {
+
+const void* main_kernel_bs(int layout, bool lut_smem) {
+  return main_instance<false, true>(layout, lut_smem);
+}
+
+}  // namespace isp_b200
