@@ -9,7 +9,143 @@
 namespace isp_b200 {
 namespace {
 
+__host__ __device__ constexpr int awb_box_bytes(int fmt) {
+  return fmt == kRawU8 ? 64 : fmt == kRawU16 ? 128 : fmt == kRawRaw10 ? 80 : 96;
+}
+
 // ---- White balance statistics ----------------------------------------------
+
+// Units of two complete quads (4 samples across, 2 rows) of one tile: the
+// white balance sums (white_balance_quad, isp_math.hpp:311-332) into 32-bit
+// per-tile sums (at most 8 samples of 2^22 per colour and thread) and, for
+// white patch, the block's bins.
+template <int kFmt, int kSrc, bool kWhitePatch, int kPat>
+__device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box, int box_bytes, int x0, int y0,
+                                         const LscTile& lt, const int* row_k, const float* row_ty,
+                                         const float* table, const float (&black)[4], const float (&inv)[4],
+                                         unsigned int* hist, unsigned int (&sum)[3], unsigned int& quads) {
+  const int quads_x = p.width / 2;
+  const int quads_y = p.height / 2;
+  const unsigned int white = static_cast<unsigned int>(p.white);
+  for (int unit = threadIdx.x; unit < 512; unit += kThreads) {
+    const int a = unit >> 4;
+    const int u = unit & 15;
+    const int qy = (y0 >> 1) + a;
+    const int qx0 = (x0 >> 1) + 2 * u;
+    if (qy >= quads_y || qx0 >= quads_x) continue;
+    unsigned int top[4], bot[4];
+    if constexpr (kSrc == 0) {
+      const uint8_t* r0 = box + (2 * a) * box_bytes;
+      const uint8_t* r1 = r0 + box_bytes;
+      if constexpr (kFmt == kRawU8) {
+        const unsigned int w0 = *reinterpret_cast<const unsigned int*>(r0 + 4 * u);
+        const unsigned int w1 = *reinterpret_cast<const unsigned int*>(r1 + 4 * u);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          top[k] = (w0 >> (8 * k)) & 0xFFU;
+          bot[k] = (w1 >> (8 * k)) & 0xFFU;
+        }
+      } else if constexpr (kFmt == kRawU16) {
+        const uint2 w0 = *reinterpret_cast<const uint2*>(r0 + 8 * u);
+        const uint2 w1 = *reinterpret_cast<const uint2*>(r1 + 8 * u);
+        top[0] = w0.x & 0xFFFFU; top[1] = w0.x >> 16; top[2] = w0.y & 0xFFFFU; top[3] = w0.y >> 16;
+        bot[0] = w1.x & 0xFFFFU; bot[1] = w1.x >> 16; bot[2] = w1.y & 0xFFFFU; bot[3] = w1.y >> 16;
+      } else {
+        // unpack4 reads sample x0 - 4 + 4u' from a box starting 16 bytes
+        // before x0; this box starts at x0: step the row back 16 bytes, u' = u + 1.
+        unpack4(kFmt, r0 - 16, u + 1, top);
+        unpack4(kFmt, r1 - 16, u + 1, bot);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int x = x0 + 4 * u + k;
+        top[k] = x < p.width ? static_cast<unsigned int>(load_raw(p, x, y0 + 2 * a)) : 0U;
+        bot[k] = x < p.width ? static_cast<unsigned int>(load_raw(p, x, y0 + 2 * a + 1)) : 0U;
+      }
+    }
+    // Linear values before white balance, capped at 4 (isp_math.hpp:320-330).
+    float v[2][4];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const unsigned int* s = r == 0 ? top : bot;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int q = (r << 1) | (k & 1);
+        v[r][k] = fmaxf(fmul(fsub(magic_to_float(s[k] | kTwo23Bits), black[q]), inv[q]), 0.0F);
+      }
+    }
+    if (lt.rows > 0) {
+      if (lt.rows <= kLscTableRows) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const int rj = 2 * a + r;
+          const int kk = row_k[rj];
+          const float tyj = row_ty[rj];
+          const int pl = p.lsc_channels == 4 ? r : 0;
+          const float4 t0 = *reinterpret_cast<const float4*>(table + (kk * 2 + pl) * kSW + 4 * u);
+          const float4 t1 = *reinterpret_cast<const float4*>(table + ((kk + 1) * 2 + pl) * kSW + 4 * u);
+          v[r][0] = fmul(v[r][0], fadd(t0.x, fmul(fsub(t1.x, t0.x), tyj)));
+          v[r][1] = fmul(v[r][1], fadd(t0.y, fmul(fsub(t1.y, t0.y), tyj)));
+          v[r][2] = fmul(v[r][2], fadd(t0.z, fmul(fsub(t1.z, t0.z), tyj)));
+          v[r][3] = fmul(v[r][3], fadd(t0.w, fmul(fsub(t1.w, t0.w), tyj)));
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            v[r][k] = fmul(v[r][k], lens_shading_gain(p, p.lsc, x0 + 4 * u + k, y0 + 2 * a + r,
+                                                      cfa_of(kPat, (r << 1) | (k & 1))));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      // A quad with a sample at or above white counts for nothing (isp_math.hpp:316-318).
+      const bool ok = qx0 + q < quads_x && top[2 * q] < white && top[2 * q + 1] < white && bot[2 * q] < white &&
+                      bot[2 * q + 1] < white;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int r = k >> 1;
+        const float x = fminf(v[r][2 * q + (k & 1)], 4.0F);
+        const unsigned int fixed = magic_int(magic_trunc(fadd(fmul(x, kFixedOne), 0.5F)));
+        sum[color_of(cfa_of(kPat, k))] += ok ? fixed : 0U;
+        if constexpr (kWhitePatch) {
+          const unsigned int bin = magic_int(magic_trunc(fmul(x, static_cast<float>(kAwbBins))));
+          if (ok) atomicAdd(&hist[color_of(cfa_of(kPat, k)) * kAwbBins + (bin < kAwbBins - 1 ? bin : kAwbBins - 1)], 1U);
+        }
+      }
+      quads += ok ? 1U : 0U;
+    }
+  }
+}
+
+template <int kSrc, bool kWhitePatch, int kPat>
+__device__ __forceinline__ void awb_tile_fmt(const FrameDesc& p, const uint8_t* box, int box_bytes, int x0, int y0,
+                                             const LscTile& lt, const int* row_k, const float* row_ty,
+                                             const float* table, const float (&black)[4], const float (&inv)[4],
+                                             unsigned int* hist, unsigned int (&sum)[3], unsigned int& quads) {
+  if constexpr (kSrc == 1) {
+    awb_tile<kRawU8, 1, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
+  } else {
+    switch (p.raw_format) {
+      case kRawU8:
+        awb_tile<kRawU8, 0, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
+        break;
+      case kRawU16:
+        awb_tile<kRawU16, 0, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
+        break;
+      case kRawRaw10:
+        awb_tile<kRawRaw10, 0, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
+        break;
+      default:
+        awb_tile<kRawRaw12, 0, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
+        break;
+    }
+  }
+}
 
 template <bool kWhitePatch, int kPat>
 __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant__ CUtensorMap map, FrameDesc p,
@@ -17,15 +153,15 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
   constexpr int kBoxRows = 64;
-  uint8_t* box = smem;                                                  // [64][box bytes]
-  float* table = reinterpret_cast<float*>(smem + 64 * 128);             // [kLscTableRows][2][kSW]
+  uint8_t* box = smem;                                                    // [64][box bytes]
+  float* table = reinterpret_cast<float*>(smem + 64 * 128);               // [kLscTableRows][2][kSW]
   int* col_mx = reinterpret_cast<int*>(table + kLscTableRows * 2 * kSW);  // [64] x 3
   int* col_ix = col_mx + 64;
   float* col_tx = reinterpret_cast<float*>(col_ix + 64);
-  int* row_my = reinterpret_cast<int*>(col_tx + 64);                    // [64] x 3
+  int* row_my = reinterpret_cast<int*>(col_tx + 64);                      // [64] x 3
   int* row_k = row_my + 64;
   float* row_ty = reinterpret_cast<float*>(row_k + 64);
-  unsigned int* hist = reinterpret_cast<unsigned int*>(row_ty + 64);    // [3][1024]
+  unsigned int* hist = reinterpret_cast<unsigned int*>(row_ty + 64);      // [3][1024]
   __shared__ uint64_t bar;
   __shared__ u64 red[kWarps];
   __shared__ int minmax[2];
@@ -33,28 +169,25 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   __shared__ bool last;
   Scratch* s = p.scratch;
   const int tid = threadIdx.x;
-  const int box_bytes = p.raw_format == kRawU8 ? 64 : p.raw_format == kRawU16 ? 128 : p.raw_format == kRawRaw10 ? 80 : 96;
+  const int box_bytes = awb_box_bytes(p.raw_format);
   if constexpr (kWhitePatch) {
     for (int i = tid; i < 3 * kAwbBins; i += kThreads) hist[i] = 0U;
   }
   if (tid == 0 && use_tma) mbar_init(&bar);
   __syncthreads();
-  // Per quad position: channel, colour, black, 1 / range.
   float black[4], inv[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     black[k] = p.black[cfa_of(kPat, k)];
     inv[k] = p.inv_range[cfa_of(kPat, k)];
   }
-  const int quads_x = p.width / 2;
-  const int quads_y = p.height / 2;
   u64 acc[4] = {0, 0, 0, 0};
   uint32_t phase = 0;
   int tile = blockIdx.x;
-  auto issue = [&](int t) {
+  const auto issue = [&](int t) {
     const int ty = t / tiles_x;
     const int x0 = (t - ty * tiles_x) * 64;
-    const int bx = p.raw_format == kRawU8 ? x0 : p.raw_format == kRawU16 ? x0 : p.raw_format == kRawRaw10 ? 5 * (x0 >> 2) : 3 * (x0 >> 1);
+    const int bx = p.raw_format == kRawRaw10 ? 5 * (x0 >> 2) : p.raw_format == kRawRaw12 ? 3 * (x0 >> 1) : x0;
     tma_load_2d(&map, box, &bar, bx, ty * 64, static_cast<unsigned int>(kBoxRows * box_bytes));
   };
   if (use_tma && tid == 0 && tile < tiles) issue(tile);
@@ -68,85 +201,16 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
       if (tid == 0) atomicExch(&s->error, 1);
     }
     phase ^= 1U;
-    // 2 quads (4 samples across, 2 rows) per unit; 32 row pairs x 16 units.
-    for (int unit = tid; unit < 512; unit += kThreads) {
-      const int a = unit >> 4;
-      const int u = unit & 15;
-      const int qy = (y0 >> 1) + a;
-      const int qx0 = (x0 >> 1) + 2 * u;
-      if (qy >= quads_y || qx0 >= quads_x) continue;
-      unsigned int top[4], bot[4];
-      if (use_tma) {
-        // Units of 4 samples at x0 + 4u: reuse unpack4 with its x0 - 4 origin.
-        const uint8_t* r0 = box + (2 * a) * box_bytes;
-        const uint8_t* r1 = r0 + box_bytes;
-        if (p.raw_format == kRawU8) {
-          const unsigned int w0 = *reinterpret_cast<const unsigned int*>(r0 + 4 * u);
-          const unsigned int w1 = *reinterpret_cast<const unsigned int*>(r1 + 4 * u);
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            top[k] = (w0 >> (8 * k)) & 0xFFU;
-            bot[k] = (w1 >> (8 * k)) & 0xFFU;
-          }
-        } else if (p.raw_format == kRawU16) {
-          const uint2 w0 = *reinterpret_cast<const uint2*>(r0 + 8 * u);
-          const uint2 w1 = *reinterpret_cast<const uint2*>(r1 + 8 * u);
-          top[0] = w0.x & 0xFFFFU; top[1] = w0.x >> 16; top[2] = w0.y & 0xFFFFU; top[3] = w0.y >> 16;
-          bot[0] = w1.x & 0xFFFFU; bot[1] = w1.x >> 16; bot[2] = w1.y & 0xFFFFU; bot[3] = w1.y >> 16;
-        } else {
-          // unpack4 reads sample x0 - 4 + 4u' from byte 11 + 5u' (RAW10) or
-          // 10 + 6u' (RAW12) of a box starting 16 bytes before x0; this box
-          // starts at x0, so shift the row pointer back 16 bytes: unit u' = u + 1.
-          unpack4(p.raw_format, r0 - 16, u + 1, top);
-          unpack4(p.raw_format, r1 - 16, u + 1, bot);
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int x = x0 + 4 * u + k;
-          top[k] = x < p.width ? static_cast<unsigned int>(load_raw(p, x, y0 + 2 * a)) : 0U;
-          bot[k] = x < p.width ? static_cast<unsigned int>(load_raw(p, x, y0 + 2 * a + 1)) : 0U;
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        if (qx0 + q >= quads_x) break;
-        const unsigned int raw[4] = {top[2 * q], top[2 * q + 1], bot[2 * q], bot[2 * q + 1]};
-        const bool ok = raw[0] < static_cast<unsigned int>(p.white) && raw[1] < static_cast<unsigned int>(p.white) &&
-                        raw[2] < static_cast<unsigned int>(p.white) && raw[3] < static_cast<unsigned int>(p.white);
-        if (!ok) continue;  // white_balance_quad, isp_math.hpp:311-319
-        unsigned int fixed[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int ci = 4 * u + 2 * q + (k & 1);  // column in the tile
-          const int rj = 2 * a + (k >> 1);         // row in the tile
-          float v = fmul(fsub(magic_to_float(raw[k] | kTwo23Bits), black[k]), inv[k]);
-          v = v > 0.0F ? v : 0.0F;
-          if (lt.rows > 0) {
-            float gain;
-            if (lt.rows <= kLscTableRows) {
-              const int kk = row_k[rj];
-              const int par = p.lsc_channels == 4 ? (k >> 1) : 0;
-              const float t0 = table[(kk * 2 + par) * kSW + ci];
-              const float t1 = table[((kk + 1) * 2 + par) * kSW + ci];
-              gain = fadd(t0, fmul(fsub(t1, t0), row_ty[rj]));
-            } else {
-              gain = lens_shading_gain(p, p.lsc, x0 + ci, y0 + rj, cfa_of(kPat, k));
-            }
-            v = fmul(v, gain);
-          }
-          v = v < 4.0F ? v : 4.0F;
-          fixed[k] = magic_int(magic_trunc(fadd(fmul(v, kFixedOne), 0.5F)));
-          if constexpr (kWhitePatch) {
-            const unsigned int bin = magic_int(magic_trunc(fmul(v, static_cast<float>(kAwbBins))));
-            atomicAdd(&hist[color_of(cfa_of(kPat, k)) * kAwbBins + (bin < kAwbBins - 1 ? bin : kAwbBins - 1)], 1U);
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) acc[color_of(cfa_of(kPat, k))] += fixed[k];
-        acc[3] += 1;
-      }
+    unsigned int sum[3] = {0U, 0U, 0U};
+    unsigned int quads = 0;
+    if (use_tma) {
+      awb_tile_fmt<0, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
+    } else {
+      awb_tile_fmt<1, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
     }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] += sum[k];
+    acc[3] += quads;
     __syncthreads();
     if (use_tma && tid == 0) {
       const int next = tile + gridDim.x;

@@ -724,10 +724,8 @@ __device__ __forceinline__ void finish_unit(const FrameDesc& p, const float (&rg
         // clamp01((m0 r + m1 g) + m2 b), isp_math.hpp:229-233.
         const float lin = add_sat(fadd(fmul(p.ccm[3 * k], c[0]), fmul(p.ccm[3 * k + 1], c[1])), fmul(p.ccm[3 * k + 2], c[2]));
         if (want_stats && (full || xb + dx < p.width)) {
-          // to_fixed (isp_math.hpp:245-247): the sum of the bit patterns
-          // 2^23 + trunc(lin 2^20 + 0.5); the 2^23s come off at the flush.
-          sums[k] += __float_as_uint(magic_trunc(fadd(fmul(lin, kFixedOne), 0.5F)));
-          if (k == 0) ++counted;
+          // to_fixed (isp_math.hpp:245-247): trunc(lin 2^20 + 0.5).
+          sums[k] += magic_int(magic_trunc(fadd(fmul(lin, kFixedOne), 0.5F)));
         }
         toned[dx][k] = tone_at<kLutSmem>(lut, lut_scale, lin);
       }

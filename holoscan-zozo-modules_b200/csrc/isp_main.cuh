@@ -154,8 +154,8 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
     }
 
     // C. Output units of 2x4 pixels: 32 unit rows x 16 unit columns. A
-    //    tile's statistics bit-pattern sums stay below 2^32 per thread
-    //    (16 pixels of at most 2^23 + 2^20).
+    //    tile's statistics sums stay below 2^32 per thread (16 pixels of
+    //    at most 2^20).
     unsigned int sums[3] = {0U, 0U, 0U};
     unsigned int counted = 0;
     for (int unit = tid; unit < 512; unit += kThreads) {
@@ -241,9 +241,6 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
     counted_total += counted;
     __syncthreads();  // the next tile overwrites the tables, S and C
   }
-  // The sums hold 2^23 + trunc(.) per counted value: take the 2^23s off.
-#pragma unroll
-  for (int k = 0; k < 3; ++k) acc[k] -= counted_total * static_cast<u64>(kTwo23Bits);
   main_finish(p, sc, acc, gains, want_stats, want_hist, hist, red, &last);
 }
 
