@@ -153,8 +153,8 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
   constexpr int kBoxRows = 64;
-  uint8_t* box = smem;                                                    // [64][box bytes]
-  float* table = reinterpret_cast<float*>(smem + 64 * 128);               // [kLscTableRows][2][kSW]
+  uint8_t* boxes = smem;                                                  // [2][64][128]: double buffer
+  float* table = reinterpret_cast<float*>(smem + 2 * 64 * 128);           // [kLscTableRows][2][kSW]
   int* col_mx = reinterpret_cast<int*>(table + kLscTableRows * 2 * kSW);  // [64] x 3
   int* col_ix = col_mx + 64;
   float* col_tx = reinterpret_cast<float*>(col_ix + 64);
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   int* row_k = row_my + 64;
   float* row_ty = reinterpret_cast<float*>(row_k + 64);
   unsigned int* hist = reinterpret_cast<unsigned int*>(row_ty + 64);      // [3][1024]
-  __shared__ uint64_t bar;
+  __shared__ uint64_t bars[2];
   __shared__ u64 red[kWarps];
   __shared__ int minmax[2];
   __shared__ int first;
@@ -173,7 +173,10 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   if constexpr (kWhitePatch) {
     for (int i = tid; i < 3 * kAwbBins; i += kThreads) hist[i] = 0U;
   }
-  if (tid == 0 && use_tma) mbar_init(&bar);
+  if (tid == 0 && use_tma) {
+    mbar_init(&bars[0]);
+    mbar_init(&bars[1]);
+  }
   __syncthreads();
   float black[4], inv[4];
 #pragma unroll
@@ -182,25 +185,33 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
     inv[k] = p.inv_range[cfa_of(kPat, k)];
   }
   u64 acc[4] = {0, 0, 0, 0};
-  uint32_t phase = 0;
+  uint32_t phases = 0;  // bit b: parity of buffer b's next completion
+  int buf = 0;
   int tile = blockIdx.x;
-  const auto issue = [&](int t) {
+  const auto issue = [&](int t, int b) {
     const int ty = t / tiles_x;
     const int x0 = (t - ty * tiles_x) * 64;
     const int bx = p.raw_format == kRawRaw10 ? 5 * (x0 >> 2) : p.raw_format == kRawRaw12 ? 3 * (x0 >> 1) : x0;
-    tma_load_2d(&map, box, &bar, bx, ty * 64, static_cast<unsigned int>(kBoxRows * box_bytes));
+    tma_load_2d(&map, boxes + b * 64 * 128, &bars[b], bx, ty * 64, static_cast<unsigned int>(kBoxRows * box_bytes));
   };
-  if (use_tma && tid == 0 && tile < tiles) issue(tile);
+  if (use_tma && tid == 0 && tile < tiles) issue(tile, 0);
   for (; tile < tiles; tile += gridDim.x) {
     const int ty = tile / tiles_x;
     const int x0 = (tile - ty * tiles_x) * 64;
     const int y0 = ty * 64;
+    // The other buffer was read by the previous tile (the block synchronised
+    // since): load the next tile into it while this one is summed.
+    if (use_tma && tid == 0 && tile + static_cast<int>(gridDim.x) < tiles) {
+      fence_async_shared();
+      issue(tile + gridDim.x, buf ^ 1);
+    }
     const LscTile lt = build_lsc(p, kPat, x0, 64, y0, 64, false, 0, 0, col_mx, col_ix, col_tx, row_my, row_k,
                                  row_ty, table, minmax);
-    if (use_tma && !mbar_wait(&bar, phase)) {
+    if (use_tma && !mbar_wait(&bars[buf], (phases >> buf) & 1U)) {
       if (tid == 0) atomicExch(&s->error, 1);
     }
-    phase ^= 1U;
+    phases ^= 1U << buf;
+    const uint8_t* box = boxes + buf * 64 * 128;
     unsigned int sum[3] = {0U, 0U, 0U};
     unsigned int quads = 0;
     if (use_tma) {
@@ -212,13 +223,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
     for (int k = 0; k < 3; ++k) acc[k] += sum[k];
     acc[3] += quads;
     __syncthreads();
-    if (use_tma && tid == 0) {
-      const int next = tile + gridDim.x;
-      if (next < tiles) {
-        fence_async_shared();
-        issue(next);
-      }
-    }
+    buf ^= 1;
   }
   // Flush: block sums, then one atomic per sum and per non-empty bin.
 #pragma unroll

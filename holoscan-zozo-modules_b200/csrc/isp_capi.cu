@@ -12,7 +12,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -238,6 +240,26 @@ bool encode_raw_map(const FrameDesc& d, int box_row_bytes, int box_rows, CUtenso
   return true;
 }
 
+cudaError_t blocks_per_sm(LaunchShapes& shapes, const void* kernel, size_t smem_max, size_t smem, int* blocks) {
+  std::lock_guard<std::mutex> lock(g_shapes_mutex);
+  if (shapes.configured.count(kernel) == 0) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_max));
+    if (e != cudaSuccess) return e;
+    shapes.configured.insert(kernel);
+  }
+  const auto key = std::make_pair(kernel, smem);
+  auto it = shapes.occupancy.find(key);
+  if (it == shapes.occupancy.end()) {
+    int n = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kernel_threads(), smem);
+    if (e != cudaSuccess) return e;
+    it = shapes.occupancy.emplace(key, n > 0 ? n : 1).first;
+  }
+  *blocks = it->second;
+  return cudaSuccess;
+}
+
 cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes& shapes, cudaStream_t stream,
                          cudaEvent_t before_main, cudaEvent_t after_main) {
   const int threads = kernel_threads();
@@ -245,14 +267,10 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
   if (d.auto_wb) {
     const bool white_patch = p.white_balance == ISP_WB_WHITE_PATCH;
     const void* k = awb_kernel(white_patch, pattern);
-    int& bpsm = shapes.awb_blocks_per_sm[white_patch ? 1 : 0][pattern];
     const size_t smem = awb_kernel_smem();
-    if (bpsm == 0) {
-      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k, threads, smem);
-      if (e != cudaSuccess) return e;
-      bpsm = std::max(bpsm, 1);
-    }
+    int bpsm = 0;
+    const cudaError_t e = blocks_per_sm(shapes, k, smem, smem, &bpsm);
+    if (e != cudaSuccess) return e;
     alignas(64) CUtensorMap map;
     int use_tma = encode_raw_map(d, awb_box_row_bytes(d.raw_format), 64, &map) ? 1 : 0;
     int tiles_x = 0;
@@ -271,16 +289,11 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
   int lut_in_smem = d.tone_size <= kLutSmemEntries && with_lut <= kSmemPerTwoCtas ? 1 : 0;
   const size_t need = lut_in_smem ? with_lut : without_lut;
   const void* k = main_kernel(malvar, sharpen, pattern, lut_in_smem != 0);
-  int& bpsm = shapes.main_blocks_per_sm[malvar][sharpen][d.out_format][pattern][lut_in_smem];
-  size_t& smem = shapes.main_smem[malvar][sharpen][d.out_format][pattern][lut_in_smem];
-  if (bpsm == 0 || smem < need) {
-    // Sized for the largest shared footprint this instance has met.
-    smem = std::max(smem, need);
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k, threads, smem);
-    if (e != cudaSuccess) return e;
-    bpsm = std::max(bpsm, 1);
-  }
+  // The instance's attribute covers its largest footprint (uint16 boxes, a
+  // full shared tone table), so frames of any format can share it.
+  const size_t most = main_kernel_smem(sharpen, kRawU16, lut_in_smem ? kLutSmemEntries : 0);
+  int bpsm = 0;
+  if (const cudaError_t e = blocks_per_sm(shapes, k, most, need, &bpsm); e != cudaSuccess) return e;
   alignas(64) CUtensorMap map;
   int use_tma = encode_raw_map(d, main_box_row_bytes(d.raw_format), main_box_rows(sharpen), &map) ? 1 : 0;
   int tiles_x = 0;

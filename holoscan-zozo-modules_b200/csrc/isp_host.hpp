@@ -6,6 +6,8 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <map>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -68,10 +70,13 @@ FrameDesc make_desc(const isp_params_c& p, const DeviceState& state, const isp_r
 // Launch shapes, per device, cached.
 struct LaunchShapes {
   int sm_count = 0;
-  int main_blocks_per_sm[2][2][4][4][2] = {};  // [malvar][sharpen][out][pattern][lut in smem]
-  size_t main_smem[2][2][4][4][2] = {};
-  int awb_blocks_per_sm[2][4] = {};  // [white patch][pattern]
+  std::set<const void*> configured;                         // kernels whose smem attribute is set
+  std::map<std::pair<const void*, size_t>, int> occupancy;  // (kernel, dynamic smem) -> CTAs per SM
 };
+
+// CTAs per SM of `kernel` at `smem` bytes of dynamic shared memory; on first
+// use sets the kernel's limit to `smem_max`. Thread-safe.
+cudaError_t blocks_per_sm(LaunchShapes& shapes, const void* kernel, size_t smem_max, size_t smem, int* blocks);
 
 // Dynamic shared memory that still lets two CTAs of the fused kernel share an
 // SM (228 KB per SM, 1 KB reserved per CTA, static shared memory).
