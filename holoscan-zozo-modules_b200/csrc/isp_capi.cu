@@ -261,7 +261,8 @@ cudaError_t blocks_per_sm(LaunchShapes& shapes, const void* kernel, size_t smem_
 }
 
 cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes& shapes, cudaStream_t stream,
-                         cudaEvent_t before_main, cudaEvent_t after_main) {
+                         cudaEvent_t before_main, cudaEvent_t after_main, const char** step) {
+  *step = "launch";
   const int threads = kernel_threads();
   const int pattern = d.pattern;
   if (d.auto_wb) {
@@ -269,6 +270,7 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
     const void* k = awb_kernel(white_patch, pattern);
     const size_t smem = awb_kernel_smem();
     int bpsm = 0;
+    *step = "white balance kernel attributes";
     const cudaError_t e = blocks_per_sm(shapes, k, smem, smem, &bpsm);
     if (e != cudaSuccess) return e;
     alignas(64) CUtensorMap map;
@@ -278,8 +280,9 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
     const int blocks = std::max(1, std::min(tiles, shapes.sm_count * bpsm));
     FrameDesc desc = d;
     void* args[] = {&map, &desc, &tiles_x, &tiles, &use_tma};
-    const cudaError_t e = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, smem, stream);
-    if (e != cudaSuccess) return e;
+    *step = "white balance kernel launch";
+    const cudaError_t e2 = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, smem, stream);
+    if (e2 != cudaSuccess) return e2;
   }
   const bool malvar = p.demosaic == ISP_DEMOSAIC_MALVAR;
   const bool sharpen = p.sharpen > 0.0F;
@@ -293,6 +296,7 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
   // full shared tone table), so frames of any format can share it.
   const size_t most = main_kernel_smem(sharpen, kRawU16, lut_in_smem ? kLutSmemEntries : 0);
   int bpsm = 0;
+  *step = "tile kernel attributes";
   if (const cudaError_t e = blocks_per_sm(shapes, k, most, need, &bpsm); e != cudaSuccess) return e;
   alignas(64) CUtensorMap map;
   int use_tma = encode_raw_map(d, main_box_row_bytes(d.raw_format), main_box_rows(sharpen), &map) ? 1 : 0;
@@ -305,6 +309,7 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
     const cudaError_t e = cudaEventRecord(before_main, stream);
     if (e != cudaSuccess) return e;
   }
+  *step = "tile kernel launch";
   const cudaError_t e = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, need, stream);
   if (e != cudaSuccess || after_main == nullptr) return e;
   return cudaEventRecord(after_main, stream);
@@ -457,9 +462,10 @@ int isp_b200_process(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp
     error = cudaStreamWaitEvent(stream, pl->done, 0);
     if (error != cudaSuccess) return fail_cuda(error, "cudaStreamWaitEvent");
   }
-  error = launch_frame(d, pl->params.c, shapes, stream, pl->before_main, pl->after_main);
+  const char* step = "launch";
+  error = launch_frame(d, pl->params.c, shapes, stream, pl->before_main, pl->after_main, &step);
   if (error == cudaSuccess) error = cudaGetLastError();
-  if (error != cudaSuccess) return fail_cuda(error, "IspPipeline (cuda)");
+  if (error != cudaSuccess) return fail_cuda(error, (std::string("IspPipeline (cuda) ") + step).c_str());
   error = cudaEventRecord(pl->done, stream);
   if (error != cudaSuccess) return fail_cuda(error, "cudaEventRecord");
   pl->queued = true;

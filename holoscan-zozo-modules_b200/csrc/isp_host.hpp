@@ -89,7 +89,8 @@ bool encode_raw_map(const FrameDesc& d, int box_row_bytes, int box_rows, CUtenso
 
 // Queues one frame's kernels on `stream` (no host synchronisation).
 // before_main / after_main (may be null) are recorded around the fused tile kernel.
+// `step` names the call that failed.
 cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes& shapes, cudaStream_t stream,
-                         cudaEvent_t before_main = nullptr, cudaEvent_t after_main = nullptr);
+                         cudaEvent_t before_main, cudaEvent_t after_main, const char** step);
 
 }  // namespace isp_b200
