@@ -186,6 +186,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   }
   u64 acc[4] = {0, 0, 0, 0};
   uint32_t phases = 0;  // bit b: parity of buffer b's next completion
+  unsigned int done = 0;  // tiles this CTA summed
   int buf = 0;
   int tile = blockIdx.x;
   const auto issue = [&](int t, int b) {
@@ -224,6 +225,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
     acc[3] += quads;
     __syncthreads();
     buf ^= 1;
+    ++done;
   }
   // Flush: block sums, then one atomic per sum and per non-empty bin.
 #pragma unroll
@@ -247,7 +249,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   }
   __threadfence();
   __syncthreads();
-  if (tid == 0) last = atomicAdd(&s->awb_done, 1U) == gridDim.x - 1;
+  if (tid == 0) last = atomicAdd(&s->awb_done, done) + done == static_cast<unsigned int>(tiles);
   __syncthreads();
   if (!last) return;
   __threadfence();

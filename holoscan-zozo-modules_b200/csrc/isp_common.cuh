@@ -532,46 +532,6 @@ __device__ void finish_stats(const FrameDesc& p, const u64 sum[3], u64 saturated
   out[11] = static_cast<float>(static_cast<double>(saturated) / static_cast<double>(pixels));
 }
 
-// The main pass's flush: block sums and histogram into the scratch, then the
-// last CTA writes the user's histogram and statistics and clears the scratch.
-__device__ void main_finish(const FrameDesc& p, Scratch* sc, const u64 (&acc)[4], const float gains[3],
-                            bool want_stats, bool want_hist, unsigned int* hist, u64* red, bool* last) {
-  const int tid = threadIdx.x;
-  if (!want_stats && !want_hist) return;
-  if (want_stats) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const u64 total = block_sum(acc[k], red);
-      if (tid == 0 && total != 0) atomicAdd(k < 3 ? &sc->sum[k] : &sc->saturated, total);
-    }
-  }
-  if (want_hist) {
-    __syncthreads();
-    for (int i = tid; i < kHistChannels * kHistBins; i += kThreads) {
-      if (hist[i] != 0U) atomicAdd(&sc->hist[i], hist[i]);
-    }
-  }
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) *last = atomicAdd(&sc->main_done, 1U) == gridDim.x - 1;
-  __syncthreads();
-  if (!*last) return;
-  __threadfence();
-  if (want_hist) {
-    for (int i = tid; i < kHistChannels * kHistBins; i += kThreads) {
-      p.hist_out[i] = __ldcg(&sc->hist[i]);
-      sc->hist[i] = 0U;
-    }
-  }
-  if (want_stats && tid == 0) {
-    const u64 sum[3] = {__ldcg(&sc->sum[0]), __ldcg(&sc->sum[1]), __ldcg(&sc->sum[2])};
-    finish_stats(p, sum, __ldcg(&sc->saturated), gains);
-    sc->sum[0] = sc->sum[1] = sc->sum[2] = 0;
-    sc->saturated = 0;
-  }
-  if (tid == 0) sc->main_done = 0;
-}
-
 template <bool kMalvar, int kPat>
 __device__ __forceinline__ void demosaic_at(const float (&w)[6][8], int dy, int dx, float rgb[3]) {
   float n[5][5];

@@ -1,12 +1,306 @@
-// isp_main.cuh - the fused tile kernel of the B200 ISP, as a template; each
-// isp_main_*.cu translation unit instantiates one demosaic method and
-// sharpening setting, so the instances compile in parallel.
+// isp_main.cuh - the fused tile pass of the B200 ISP as device templates: a
+// frame's per-CTA setup, one 64x64 tile (phases A, B, C), and the per-frame
+// flush with the last-tile finish. The single-frame kernel here and the
+// batch kernel (isp_batch.cu) are both built from them, so every frame gets
+// the same arithmetic however it is launched. Each isp_main_*.cu
+// translation unit instantiates one demosaic method and sharpening setting,
+// so the instances compile in parallel.
 #pragma once
 
 #include "isp_common.cuh"
 
 namespace isp_b200 {
 namespace {
+
+// Shared memory of a CTA, carved from one dynamic allocation.
+struct TileSmem {
+  uint8_t* box;
+  float* S;
+  float2* Crg;
+  float* Cb;
+  float* table;
+  int* col_mx;
+  int* col_ix;
+  float* col_tx;
+  int* row_my;
+  int* row_k;
+  float* row_ty;
+  unsigned int* hist;
+  float2* lut_s;
+};
+
+__device__ __forceinline__ TileSmem carve(unsigned char* smem, const Layout& L, int sample_rows) {
+  TileSmem m;
+  m.box = smem + L.raw;
+  m.S = reinterpret_cast<float*>(smem + L.samples);
+  m.Crg = reinterpret_cast<float2*>(smem + L.rg);
+  m.Cb = reinterpret_cast<float*>(smem + L.b);
+  m.table = reinterpret_cast<float*>(smem + L.lsc);
+  m.col_mx = reinterpret_cast<int*>(smem + L.cols);
+  m.col_ix = m.col_mx + kSW;
+  m.col_tx = reinterpret_cast<float*>(m.col_ix + kSW);
+  m.row_my = reinterpret_cast<int*>(smem + L.rows);
+  m.row_k = m.row_my + sample_rows;
+  m.row_ty = reinterpret_cast<float*>(m.row_k + sample_rows);
+  m.hist = reinterpret_cast<unsigned int*>(smem + L.hist);
+  m.lut_s = reinterpret_cast<float2*>(smem + L.lut);
+  return m;
+}
+
+// What every tile of a frame reads, set up once per frame by a CTA.
+struct FrameSetup {
+  float gains[3];  // the white balance the frame is processed with
+  float qblack[4];  // per quad position
+  float qinv[4];
+  float qgain[4];
+  const float2* lut;
+  float lut_scale;
+  bool swap_rb;
+  bool want_hist;
+  bool want_stats;
+};
+
+// Reads the frame's gains (its estimate, for auto white balance), copies the
+// tone table to shared memory (kLutSmem) and clears the block histogram.
+// The caller synchronises the block before the first tile.
+template <bool kLutSmem>
+__device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const TileSmem& m) {
+  FrameSetup f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) f.gains[k] = p.auto_wb ? __ldcg(&p.scratch->awb_gains[k]) : p.wb[k];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int ch = p.cfa[k];
+    f.qblack[k] = p.black[ch];
+    f.qinv[k] = p.inv_range[ch];
+    f.qgain[k] = f.gains[color_of(ch)];
+  }
+  f.lut = p.tone;
+  if constexpr (kLutSmem) {
+    for (int i = threadIdx.x; i < p.tone_size; i += kThreads) m.lut_s[i] = p.tone[i];
+    f.lut = m.lut_s;
+  }
+  f.lut_scale = static_cast<float>(p.tone_size - 1);
+  // The demosaic runs as the layout's canonical pattern (RGGB or GRBG); for
+  // BGGR and GBRG its red and blue outputs trade places before the colour
+  // matrix (the estimates' arithmetic is the same at either site).
+  f.swap_rb = (p.pattern & 1) != 0;
+  f.want_hist = p.hist_out != nullptr;
+  f.want_stats = p.stats_out != nullptr;
+  if (f.want_hist) {
+    for (int i = threadIdx.x; i < kHistChannels * kHistBins; i += kThreads) m.hist[i] = 0U;
+  }
+  return f;
+}
+
+// One 64x64 tile at (x0, y0). `map` is the frame's TMA descriptor (its box
+// is waited for on `bar`); after phase A, when the box is free again,
+// `after_a()` runs (to prefetch the next tile). Adds the tile's statistics
+// sums and saturated count to `acc` (per thread).
+template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, class AfterA>
+__device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f, const TileSmem& m, int* minmax,
+                                         int x0, int y0, bool use_tma, uint64_t* bar, uint32_t& phase,
+                                         u64 (&acc)[4], AfterA after_a) {
+  using G = Geom<kSharpen>;
+  constexpr int kPat = kLayout * 2;
+  const int tid = threadIdx.x;
+  const int box_bytes = box_row_bytes(p.raw_format);
+  const bool interior = x0 >= 4 && y0 >= G::kHalo && x0 + kSW - 4 <= p.width && y0 + kTH + G::kHalo <= p.height;
+  TileCtx t;
+  t.x0 = x0;
+  t.y0 = y0;
+  t.box = m.box;
+  t.col_mx = m.col_mx;
+  t.row_my = m.row_my;
+  t.row_k = m.row_k;
+  t.row_ty = m.row_ty;
+  t.table = m.table;
+  t.lt = build_lsc(p, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, !interior, p.width + 3, p.height + G::kHalo - 1,
+                   m.col_mx, m.col_ix, m.col_tx, m.row_my, m.row_k, m.row_ty, m.table, minmax);
+  if (use_tma && !mbar_wait(bar, phase)) {
+    if (tid == 0) atomicExch(&p.scratch->error, 1);
+  }
+  phase ^= 1U;
+
+  // A. Samples of the tile and its halo, preprocessed once.
+  unsigned int saturated;
+  if (!use_tma) {
+    saturated = phase_a_fmt<2, G::kHalo>(p, t, m.S, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
+  } else if (interior) {
+    saturated = phase_a_fmt<0, G::kHalo>(p, t, m.S, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
+  } else {
+    saturated = phase_a_fmt<1, G::kHalo>(p, t, m.S, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
+  }
+  acc[3] += saturated;
+  __syncthreads();
+  after_a();
+
+  // B. (Sharpening) RGB of the tile and a one-pixel ring, 2x4 pixels a
+  //    unit; outside the image these are the reference's virtual pixels
+  //    (cpu_pipeline.cpp:22-46).
+  if constexpr (kSharpen) {
+    constexpr int kUnitsB = 17 * 34;
+    for (int unit = tid; unit < kUnitsB; unit += kThreads) {
+      const int qr = unit / 17;
+      const int qc = unit - qr * 17;
+      float w[6][8];
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        const float4 a = *reinterpret_cast<const float4*>(m.S + (2 * qr + r) * kSW + 4 * qc);
+        const float4 b = *reinterpret_cast<const float4*>(m.S + (2 * qr + r) * kSW + 4 * qc + 4);
+        w[r][0] = a.x; w[r][1] = a.y; w[r][2] = a.z; w[r][3] = a.w;
+        w[r][4] = b.x; w[r][5] = b.y; w[r][6] = b.z; w[r][7] = b.w;
+      }
+      const bool inner = qr >= 1 && qr <= 32 && qc >= 1 && qc <= 15;
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy) {
+        const int cy = 2 * qr + dy - 1;
+#pragma unroll
+        for (int dx = 0; dx < 4; ++dx) {
+          const int cx = 4 * qc + dx - 1;
+          if (!inner && (cy < 0 || cy >= G::kCH || cx < 0 || cx >= kTW + 2)) continue;
+          float rgb[3];
+          demosaic_at<kMalvar, kPat>(w, dy, dx, rgb);
+          m.Crg[cy * G::kCW + cx] = make_float2(rgb[0], rgb[1]);
+          m.Cb[cy * G::kCW + cx] = rgb[2];
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // C. Output units of 2x4 pixels: 32 unit rows x 16 unit columns. A
+  //    tile's statistics sums stay below 2^32 per thread (16 pixels of at
+  //    most 2^20).
+  unsigned int sums[3] = {0U, 0U, 0U};
+  unsigned int counted = 0;
+  for (int unit = tid; unit < 512; unit += kThreads) {
+    const int ur = unit >> 4;
+    const int uc = unit & 15;
+    float rgb[2][4][3];
+    if constexpr (kSharpen) {
+      // 3x3 neighbourhoods from the RGB planes: window rows 2ur..2ur+3,
+      // columns 4uc..4uc+5 (pixel x0 + 4uc + dx sits at column 4uc + dx + 1).
+      float mm[4][6][3];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const float2* rg = m.Crg + (2 * ur + r) * G::kCW + 4 * uc;
+        const float4 a = *reinterpret_cast<const float4*>(rg);
+        const float4 b = *reinterpret_cast<const float4*>(rg + 2);
+        const float4 c = *reinterpret_cast<const float4*>(rg + 4);
+        mm[r][0][0] = a.x; mm[r][0][1] = a.y; mm[r][1][0] = a.z; mm[r][1][1] = a.w;
+        mm[r][2][0] = b.x; mm[r][2][1] = b.y; mm[r][3][0] = b.z; mm[r][3][1] = b.w;
+        mm[r][4][0] = c.x; mm[r][4][1] = c.y; mm[r][5][0] = c.z; mm[r][5][1] = c.w;
+        const float* bp = m.Cb + (2 * ur + r) * G::kCW + 4 * uc;
+        const float4 d = *reinterpret_cast<const float4*>(bp);
+        const float2 e = *reinterpret_cast<const float2*>(bp + 4);
+        mm[r][0][2] = d.x; mm[r][1][2] = d.y; mm[r][2][2] = d.z; mm[r][3][2] = d.w;
+        mm[r][4][2] = e.x; mm[r][5][2] = e.y;
+      }
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy) {
+#pragma unroll
+        for (int dx = 0; dx < 4; ++dx) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            rgb[dy][dx][k] = sharpen_one(mm[dy + 1][dx + 1][k], mm[dy][dx + 1][k], mm[dy + 2][dx + 1][k],
+                                         mm[dy + 1][dx][k], mm[dy + 1][dx + 2][k], mm[dy][dx][k], mm[dy][dx + 2][k],
+                                         mm[dy + 2][dx][k], mm[dy + 2][dx + 2][k], p.sharpen);
+          }
+        }
+      }
+    } else {
+      // Samples rows 2ur .. 2ur + 5 (halo 2), columns 4uc + 2 .. 4uc + 9.
+      float w[6][8];
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        if (!kMalvar && (r == 0 || r == 5)) {
+#pragma unroll
+          for (int c = 0; c < 8; ++c) w[r][c] = 0.0F;
+          continue;
+        }
+        const float* row = m.S + (2 * ur + r) * kSW + 4 * uc;
+        const float4 a = *reinterpret_cast<const float4*>(row);
+        const float4 b = *reinterpret_cast<const float4*>(row + 4);
+        const float4 c = *reinterpret_cast<const float4*>(row + 8);
+        w[r][0] = a.z; w[r][1] = a.w; w[r][2] = b.x; w[r][3] = b.y;
+        w[r][4] = b.z; w[r][5] = b.w; w[r][6] = c.x; w[r][7] = c.y;
+      }
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy) {
+#pragma unroll
+        for (int dx = 0; dx < 4; ++dx) demosaic_at<kMalvar, kPat>(w, dy, dx, rgb[dy][dx]);
+      }
+    }
+    const int xb = x0 + 4 * uc;
+    const int yb = y0 + 2 * ur;
+    const bool full = xb + 3 < p.width && yb + 1 < p.height;
+    if (f.swap_rb) {
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy) {
+#pragma unroll
+        for (int dx = 0; dx < 4; ++dx) {
+          const float r = rgb[dy][dx][0];
+          rgb[dy][dx][0] = rgb[dy][dx][2];
+          rgb[dy][dx][2] = r;
+        }
+      }
+    }
+    if (full) {
+      finish_unit_any<kLutSmem>(p, rgb, xb, yb, true, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist, sums,
+                                counted);
+    } else if (xb < p.width && yb < p.height) {
+      finish_unit_any<kLutSmem>(p, rgb, xb, yb, false, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist, sums,
+                                counted);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) acc[k] += sums[k];
+  __syncthreads();  // the next tile overwrites the tables, S and C
+}
+
+// The main pass's flush of one frame by one CTA, after it processed
+// `tiles_done` of the frame's `tiles_total` tiles: block sums and histogram
+// into the frame's scratch; the CTA that completes the frame's tile count
+// writes the user's histogram and statistics and clears the scratch.
+__device__ void flush_frame(const FrameDesc& p, const FrameSetup& f, const u64 (&acc)[4], unsigned int* hist,
+                            u64* red, bool* last, unsigned int tiles_done, unsigned int tiles_total) {
+  Scratch* sc = p.scratch;
+  const int tid = threadIdx.x;
+  if (!f.want_stats && !f.want_hist) return;
+  if (f.want_stats) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const u64 total = block_sum(acc[k], red);
+      if (tid == 0 && total != 0) atomicAdd(k < 3 ? &sc->sum[k] : &sc->saturated, total);
+    }
+  }
+  if (f.want_hist) {
+    __syncthreads();
+    for (int i = tid; i < kHistChannels * kHistBins; i += kThreads) {
+      if (hist[i] != 0U) atomicAdd(&sc->hist[i], hist[i]);
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) *last = atomicAdd(&sc->main_done, tiles_done) + tiles_done == tiles_total;
+  __syncthreads();
+  if (!*last) return;
+  __threadfence();
+  if (f.want_hist) {
+    for (int i = tid; i < kHistChannels * kHistBins; i += kThreads) {
+      p.hist_out[i] = __ldcg(&sc->hist[i]);
+      sc->hist[i] = 0U;
+    }
+  }
+  if (f.want_stats && tid == 0) {
+    const u64 sum[3] = {__ldcg(&sc->sum[0]), __ldcg(&sc->sum[1]), __ldcg(&sc->sum[2])};
+    finish_stats(p, sum, __ldcg(&sc->saturated), f.gains);
+    sc->sum[0] = sc->sum[1] = sc->sum[2] = 0;
+    sc->saturated = 0;
+  }
+  if (tid == 0) sc->main_done = 0;
+}
 
 template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem>
 __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_constant__ CUtensorMap map, FrameDesc p,
@@ -15,235 +309,43 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
   const int box_bytes = box_row_bytes(p.raw_format);
-  const Layout L = layout_of(kSharpen, box_bytes, kLutSmem ? p.tone_size : 0);
-  uint8_t* box = smem + L.raw;
-  float* S = reinterpret_cast<float*>(smem + L.samples);
-  float2* Crg = reinterpret_cast<float2*>(smem + L.rg);
-  float* Cb = reinterpret_cast<float*>(smem + L.b);
-  float* table = reinterpret_cast<float*>(smem + L.lsc);
-  int* col_mx = reinterpret_cast<int*>(smem + L.cols);
-  int* col_ix = col_mx + kSW;
-  float* col_tx = reinterpret_cast<float*>(col_ix + kSW);
-  int* row_my = reinterpret_cast<int*>(smem + L.rows);
-  int* row_k = row_my + G::kSH;
-  float* row_ty = reinterpret_cast<float*>(row_k + G::kSH);
-  unsigned int* hist = reinterpret_cast<unsigned int*>(smem + L.hist);
-  float2* lut_s = reinterpret_cast<float2*>(smem + L.lut);
+  const TileSmem m = carve(smem, layout_of(kSharpen, box_bytes, kLutSmem ? p.tone_size : 0), G::kSH);
   __shared__ uint64_t bar;
   __shared__ u64 red[kWarps];
   __shared__ int minmax[2];
   __shared__ bool last;
   static_cast<void>(lut_in_smem);
 
-  // The demosaic runs as the layout's canonical pattern (RGGB or GRBG); for
-  // BGGR and GBRG its red and blue outputs trade places before the colour
-  // matrix (the estimates' arithmetic is the same at either site).
-  constexpr int kPat = kLayout * 2;
-  const bool swap_rb = (p.pattern & 1) != 0;
-  const int tid = threadIdx.x;
-  Scratch* sc = p.scratch;
-  const bool want_hist = p.hist_out != nullptr;
-  const bool want_stats = p.stats_out != nullptr;
-  float gains[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) gains[k] = p.auto_wb ? __ldcg(&sc->awb_gains[k]) : p.wb[k];
-  float qblack[4], qinv[4], qgain[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int ch = p.cfa[k];
-    qblack[k] = p.black[ch];
-    qinv[k] = p.inv_range[ch];
-    qgain[k] = gains[color_of(ch)];
-  }
-  const float2* lut = p.tone;
-  if constexpr (kLutSmem) {
-    for (int i = tid; i < p.tone_size; i += kThreads) lut_s[i] = p.tone[i];
-    lut = lut_s;
-  }
-  const float lut_scale = static_cast<float>(p.tone_size - 1);
-  if (want_hist) {
-    for (int i = tid; i < kHistChannels * kHistBins; i += kThreads) hist[i] = 0U;
-  }
-  if (tid == 0 && use_tma) mbar_init(&bar);
+  const FrameSetup f = setup_frame<kLutSmem>(p, m);
+  if (threadIdx.x == 0 && use_tma) mbar_init(&bar);
   __syncthreads();
 
   const int fmt = p.raw_format;
   u64 acc[4] = {0, 0, 0, 0};  // linear R, G, B in 2^-20 units; saturated samples
-  u64 counted_total = 0;      // pixels whose bit patterns the sums hold
   uint32_t phase = 0;
-  int tile = blockIdx.x;
   const auto issue = [&](int t) {
     const int ty = t / tiles_x;
     const int x0 = (t - ty * tiles_x) * kTW;
-    tma_load_2d(&map, box, &bar, box_x(fmt, x0), ty * kTH - G::kHalo, static_cast<unsigned int>(G::kSH * box_bytes));
+    tma_load_2d(&map, m.box, &bar, box_x(fmt, x0), ty * kTH - G::kHalo, static_cast<unsigned int>(G::kSH * box_bytes));
   };
-  if (use_tma && tid == 0 && tile < tiles) issue(tile);
-
-  for (; tile < tiles; tile += gridDim.x) {
+  if (use_tma && threadIdx.x == 0 && static_cast<int>(blockIdx.x) < tiles) issue(blockIdx.x);
+  unsigned int done = 0;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const int ty = tile / tiles_x;
     const int x0 = (tile - ty * tiles_x) * kTW;
-    const int y0 = ty * kTH;
-    const bool interior = x0 >= 4 && y0 >= G::kHalo && x0 + kSW - 4 <= p.width && y0 + kTH + G::kHalo <= p.height;
-    TileCtx t;
-    t.x0 = x0;
-    t.y0 = y0;
-    t.box = box;
-    t.col_mx = col_mx;
-    t.row_my = row_my;
-    t.row_k = row_k;
-    t.row_ty = row_ty;
-    t.table = table;
-    t.lt = build_lsc(p, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, !interior, p.width + 3, p.height + G::kHalo - 1,
-                     col_mx, col_ix, col_tx, row_my, row_k, row_ty, table, minmax);
-    if (use_tma && !mbar_wait(&bar, phase)) {
-      if (tid == 0) atomicExch(&sc->error, 1);
-    }
-    phase ^= 1U;
-
-    unsigned int saturated;
-    if (!use_tma) {
-      saturated = phase_a_fmt<2, G::kHalo>(p, t, S, box_bytes, qblack, qinv, qgain, want_stats);
-    } else if (interior) {
-      saturated = phase_a_fmt<0, G::kHalo>(p, t, S, box_bytes, qblack, qinv, qgain, want_stats);
-    } else {
-      saturated = phase_a_fmt<1, G::kHalo>(p, t, S, box_bytes, qblack, qinv, qgain, want_stats);
-    }
-    acc[3] += saturated;
-    __syncthreads();
-    // The box is free: prefetch the next tile's raw samples during B and C.
-    if (use_tma && tid == 0) {
-      const int next = tile + gridDim.x;
-      if (next < tiles) {
+    // The box is free after phase A: prefetch the next tile during B and C.
+    const auto prefetch = [&] {
+      if (use_tma && threadIdx.x == 0 && tile + static_cast<int>(gridDim.x) < tiles) {
         fence_async_shared();
-        issue(next);
+        issue(tile + gridDim.x);
       }
-    }
-
-    // B. (Sharpening) RGB of the tile and a one-pixel ring, 2x4 pixels a
-    //    unit; outside the image these are the reference's virtual pixels
-    //    (cpu_pipeline.cpp:22-46).
-    if constexpr (kSharpen) {
-      constexpr int kUnitsB = 17 * 34;
-      for (int unit = tid; unit < kUnitsB; unit += kThreads) {
-        const int qr = unit / 17;
-        const int qc = unit - qr * 17;
-        float w[6][8];
-#pragma unroll
-        for (int r = 0; r < 6; ++r) {
-          const float4 a = *reinterpret_cast<const float4*>(S + (2 * qr + r) * kSW + 4 * qc);
-          const float4 b = *reinterpret_cast<const float4*>(S + (2 * qr + r) * kSW + 4 * qc + 4);
-          w[r][0] = a.x; w[r][1] = a.y; w[r][2] = a.z; w[r][3] = a.w;
-          w[r][4] = b.x; w[r][5] = b.y; w[r][6] = b.z; w[r][7] = b.w;
-        }
-        const bool inner = qr >= 1 && qr <= 32 && qc >= 1 && qc <= 15;
-#pragma unroll
-        for (int dy = 0; dy < 2; ++dy) {
-          const int cy = 2 * qr + dy - 1;
-#pragma unroll
-          for (int dx = 0; dx < 4; ++dx) {
-            const int cx = 4 * qc + dx - 1;
-            if (!inner && (cy < 0 || cy >= G::kCH || cx < 0 || cx >= kTW + 2)) continue;
-            float rgb[3];
-            demosaic_at<kMalvar, kPat>(w, dy, dx, rgb);
-            Crg[cy * G::kCW + cx] = make_float2(rgb[0], rgb[1]);
-            Cb[cy * G::kCW + cx] = rgb[2];
-          }
-        }
-      }
-      __syncthreads();
-    }
-
-    // C. Output units of 2x4 pixels: 32 unit rows x 16 unit columns. A
-    //    tile's statistics sums stay below 2^32 per thread (16 pixels of
-    //    at most 2^20).
-    unsigned int sums[3] = {0U, 0U, 0U};
-    unsigned int counted = 0;
-    for (int unit = tid; unit < 512; unit += kThreads) {
-      const int ur = unit >> 4;
-      const int uc = unit & 15;
-      float rgb[2][4][3];
-      if constexpr (kSharpen) {
-        // 3x3 neighbourhoods from the RGB planes: window rows 2ur..2ur+3,
-        // columns 4uc..4uc+5 (pixel x0 + 4uc + dx sits at column 4uc + dx + 1).
-        float m[4][6][3];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const float2* rg = Crg + (2 * ur + r) * G::kCW + 4 * uc;
-          const float4 a = *reinterpret_cast<const float4*>(rg);
-          const float4 b = *reinterpret_cast<const float4*>(rg + 2);
-          const float4 c = *reinterpret_cast<const float4*>(rg + 4);
-          m[r][0][0] = a.x; m[r][0][1] = a.y; m[r][1][0] = a.z; m[r][1][1] = a.w;
-          m[r][2][0] = b.x; m[r][2][1] = b.y; m[r][3][0] = b.z; m[r][3][1] = b.w;
-          m[r][4][0] = c.x; m[r][4][1] = c.y; m[r][5][0] = c.z; m[r][5][1] = c.w;
-          const float* bp = Cb + (2 * ur + r) * G::kCW + 4 * uc;
-          const float4 d = *reinterpret_cast<const float4*>(bp);
-          const float2 e = *reinterpret_cast<const float2*>(bp + 4);
-          m[r][0][2] = d.x; m[r][1][2] = d.y; m[r][2][2] = d.z; m[r][3][2] = d.w;
-          m[r][4][2] = e.x; m[r][5][2] = e.y;
-        }
-#pragma unroll
-        for (int dy = 0; dy < 2; ++dy) {
-#pragma unroll
-          for (int dx = 0; dx < 4; ++dx) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-              rgb[dy][dx][k] = sharpen_one(m[dy + 1][dx + 1][k], m[dy][dx + 1][k], m[dy + 2][dx + 1][k],
-                                           m[dy + 1][dx][k], m[dy + 1][dx + 2][k], m[dy][dx][k], m[dy][dx + 2][k],
-                                           m[dy + 2][dx][k], m[dy + 2][dx + 2][k], p.sharpen);
-            }
-          }
-        }
-      } else {
-        // Samples rows 2ur .. 2ur + 5 (halo 2), columns 4uc + 2 .. 4uc + 9.
-        float w[6][8];
-#pragma unroll
-        for (int r = 0; r < 6; ++r) {
-          if (!kMalvar && (r == 0 || r == 5)) {
-#pragma unroll
-            for (int c = 0; c < 8; ++c) w[r][c] = 0.0F;
-            continue;
-          }
-          const float* row = S + (2 * ur + r) * kSW + 4 * uc;
-          const float4 a = *reinterpret_cast<const float4*>(row);
-          const float4 b = *reinterpret_cast<const float4*>(row + 4);
-          const float4 c = *reinterpret_cast<const float4*>(row + 8);
-          w[r][0] = a.z; w[r][1] = a.w; w[r][2] = b.x; w[r][3] = b.y;
-          w[r][4] = b.z; w[r][5] = b.w; w[r][6] = c.x; w[r][7] = c.y;
-        }
-#pragma unroll
-        for (int dy = 0; dy < 2; ++dy) {
-#pragma unroll
-          for (int dx = 0; dx < 4; ++dx) demosaic_at<kMalvar, kPat>(w, dy, dx, rgb[dy][dx]);
-        }
-      }
-      const int xb = x0 + 4 * uc;
-      const int yb = y0 + 2 * ur;
-      const bool full = xb + 3 < p.width && yb + 1 < p.height;
-      if (swap_rb) {
-#pragma unroll
-        for (int dy = 0; dy < 2; ++dy) {
-#pragma unroll
-          for (int dx = 0; dx < 4; ++dx) {
-            const float r = rgb[dy][dx][0];
-            rgb[dy][dx][0] = rgb[dy][dx][2];
-            rgb[dy][dx][2] = r;
-          }
-        }
-      }
-      if (full) {
-        finish_unit_any<kLutSmem>(p, rgb, xb, yb, true, lut, lut_scale, want_stats, want_hist, hist, sums, counted);
-      } else if (xb < p.width && yb < p.height) {
-        finish_unit_any<kLutSmem>(p, rgb, xb, yb, false, lut, lut_scale, want_stats, want_hist, hist, sums, counted);
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) acc[k] += sums[k];
-    counted_total += counted;
-    __syncthreads();  // the next tile overwrites the tables, S and C
+    };
+    run_tile<kMalvar, kSharpen, kLayout, kLutSmem>(p, f, m, minmax, x0, ty * kTH, use_tma != 0, &bar, phase, acc,
+                                                   prefetch);
+    ++done;
   }
-  main_finish(p, sc, acc, gains, want_stats, want_hist, hist, red, &last);
+  flush_frame(p, f, acc, m.hist, red, &last, done, static_cast<unsigned int>(tiles));
 }
-
 
 template <bool kMalvar, bool kSharpen>
 const void* main_instance(int layout, bool lut_smem) {

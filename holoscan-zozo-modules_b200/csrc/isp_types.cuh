@@ -27,7 +27,7 @@ struct Scratch {
   u64 awb_sum[3];
   u64 awb_quads;
   unsigned int awb_hist[3][kAwbBins];
-  unsigned int awb_done;  // CTAs of the statistics pass that have flushed
+  unsigned int awb_done;  // tiles of the statistics pass flushed so far
   // The white balance state carried from frame to frame (isp_math.hpp:71-74).
   float awb_gains[3];
   int awb_valid;
@@ -35,7 +35,7 @@ struct Scratch {
   u64 sum[3];
   u64 saturated;
   unsigned int hist[kHistChannels * kHistBins];
-  unsigned int main_done;
+  unsigned int main_done;  // tiles of the main pass flushed so far
   int error;  // a bounded wait in a kernel gave up (1)
   unsigned int pad[2];
 };
