@@ -4,148 +4,13 @@
 // binned for white patch) in the block, then flushed once; the last CTA to
 // finish forms the frame's estimate (finish_white_balance, isp_math.hpp:357-384)
 // and clears the sums for the next frame.
-#include "isp_common.cuh"
+#include "isp_awb.cuh"
 
 namespace isp_b200 {
 namespace {
 
-__host__ __device__ constexpr int awb_box_bytes(int fmt) {
-  return fmt == kRawU8 ? 64 : fmt == kRawU16 ? 128 : fmt == kRawRaw10 ? 80 : 96;
-}
 
 // ---- White balance statistics ----------------------------------------------
-
-// Units of two complete quads (4 samples across, 2 rows) of one tile: the
-// white balance sums (white_balance_quad, isp_math.hpp:311-332) into 32-bit
-// per-tile sums (at most 8 samples of 2^22 per colour and thread) and, for
-// white patch, the block's bins.
-template <int kFmt, int kSrc, bool kWhitePatch, int kPat>
-__device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box, int box_bytes, int x0, int y0,
-                                         const LscTile& lt, const int* row_k, const float* row_ty,
-                                         const float* table, const float (&black)[4], const float (&inv)[4],
-                                         unsigned int* hist, unsigned int (&sum)[3], unsigned int& quads) {
-  const int quads_x = p.width / 2;
-  const int quads_y = p.height / 2;
-  const unsigned int white = static_cast<unsigned int>(p.white);
-  for (int unit = threadIdx.x; unit < 512; unit += kThreads) {
-    const int a = unit >> 4;
-    const int u = unit & 15;
-    const int qy = (y0 >> 1) + a;
-    const int qx0 = (x0 >> 1) + 2 * u;
-    if (qy >= quads_y || qx0 >= quads_x) continue;
-    unsigned int top[4], bot[4];
-    if constexpr (kSrc == 0) {
-      const uint8_t* r0 = box + (2 * a) * box_bytes;
-      const uint8_t* r1 = r0 + box_bytes;
-      if constexpr (kFmt == kRawU8) {
-        const unsigned int w0 = *reinterpret_cast<const unsigned int*>(r0 + 4 * u);
-        const unsigned int w1 = *reinterpret_cast<const unsigned int*>(r1 + 4 * u);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          top[k] = (w0 >> (8 * k)) & 0xFFU;
-          bot[k] = (w1 >> (8 * k)) & 0xFFU;
-        }
-      } else if constexpr (kFmt == kRawU16) {
-        const uint2 w0 = *reinterpret_cast<const uint2*>(r0 + 8 * u);
-        const uint2 w1 = *reinterpret_cast<const uint2*>(r1 + 8 * u);
-        top[0] = w0.x & 0xFFFFU; top[1] = w0.x >> 16; top[2] = w0.y & 0xFFFFU; top[3] = w0.y >> 16;
-        bot[0] = w1.x & 0xFFFFU; bot[1] = w1.x >> 16; bot[2] = w1.y & 0xFFFFU; bot[3] = w1.y >> 16;
-      } else {
-        // unpack4 reads sample x0 - 4 + 4u' from a box starting 16 bytes
-        // before x0; this box starts at x0: step the row back 16 bytes, u' = u + 1.
-        unpack4(kFmt, r0 - 16, u + 1, top);
-        unpack4(kFmt, r1 - 16, u + 1, bot);
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int x = x0 + 4 * u + k;
-        top[k] = x < p.width ? static_cast<unsigned int>(load_raw(p, x, y0 + 2 * a)) : 0U;
-        bot[k] = x < p.width ? static_cast<unsigned int>(load_raw(p, x, y0 + 2 * a + 1)) : 0U;
-      }
-    }
-    // Linear values before white balance, capped at 4 (isp_math.hpp:320-330).
-    float v[2][4];
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const unsigned int* s = r == 0 ? top : bot;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int q = (r << 1) | (k & 1);
-        v[r][k] = fmaxf(fmul(fsub(magic_to_float(s[k] | kTwo23Bits), black[q]), inv[q]), 0.0F);
-      }
-    }
-    if (lt.rows > 0) {
-      if (lt.rows <= kLscTableRows) {
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          const int rj = 2 * a + r;
-          const int kk = row_k[rj];
-          const float tyj = row_ty[rj];
-          const int pl = p.lsc_channels == 4 ? r : 0;
-          const float4 t0 = *reinterpret_cast<const float4*>(table + (kk * 2 + pl) * kSW + 4 * u);
-          const float4 t1 = *reinterpret_cast<const float4*>(table + ((kk + 1) * 2 + pl) * kSW + 4 * u);
-          v[r][0] = fmul(v[r][0], fadd(t0.x, fmul(fsub(t1.x, t0.x), tyj)));
-          v[r][1] = fmul(v[r][1], fadd(t0.y, fmul(fsub(t1.y, t0.y), tyj)));
-          v[r][2] = fmul(v[r][2], fadd(t0.z, fmul(fsub(t1.z, t0.z), tyj)));
-          v[r][3] = fmul(v[r][3], fadd(t0.w, fmul(fsub(t1.w, t0.w), tyj)));
-        }
-      } else {
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            v[r][k] = fmul(v[r][k], lens_shading_gain(p, p.lsc, x0 + 4 * u + k, y0 + 2 * a + r,
-                                                      cfa_of(kPat, (r << 1) | (k & 1))));
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      // A quad with a sample at or above white counts for nothing (isp_math.hpp:316-318).
-      const bool ok = qx0 + q < quads_x && top[2 * q] < white && top[2 * q + 1] < white && bot[2 * q] < white &&
-                      bot[2 * q + 1] < white;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int r = k >> 1;
-        const float x = fminf(v[r][2 * q + (k & 1)], 4.0F);
-        const unsigned int fixed = magic_int(magic_trunc(fadd(fmul(x, kFixedOne), 0.5F)));
-        sum[color_of(cfa_of(kPat, k))] += ok ? fixed : 0U;
-        if constexpr (kWhitePatch) {
-          const unsigned int bin = magic_int(magic_trunc(fmul(x, static_cast<float>(kAwbBins))));
-          if (ok) atomicAdd(&hist[color_of(cfa_of(kPat, k)) * kAwbBins + (bin < kAwbBins - 1 ? bin : kAwbBins - 1)], 1U);
-        }
-      }
-      quads += ok ? 1U : 0U;
-    }
-  }
-}
-
-template <int kSrc, bool kWhitePatch, int kPat>
-__device__ __forceinline__ void awb_tile_fmt(const FrameDesc& p, const uint8_t* box, int box_bytes, int x0, int y0,
-                                             const LscTile& lt, const int* row_k, const float* row_ty,
-                                             const float* table, const float (&black)[4], const float (&inv)[4],
-                                             unsigned int* hist, unsigned int (&sum)[3], unsigned int& quads) {
-  if constexpr (kSrc == 1) {
-    awb_tile<kRawU8, 1, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
-  } else {
-    switch (p.raw_format) {
-      case kRawU8:
-        awb_tile<kRawU8, 0, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
-        break;
-      case kRawU16:
-        awb_tile<kRawU16, 0, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
-        break;
-      case kRawRaw10:
-        awb_tile<kRawRaw10, 0, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
-        break;
-      default:
-        awb_tile<kRawRaw12, 0, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
-        break;
-    }
-  }
-}
 
 template <bool kWhitePatch, int kPat>
 __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant__ CUtensorMap map, FrameDesc p,
@@ -192,8 +57,8 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   const auto issue = [&](int t, int b) {
     const int ty = t / tiles_x;
     const int x0 = (t - ty * tiles_x) * 64;
-    const int bx = p.raw_format == kRawRaw10 ? 5 * (x0 >> 2) : p.raw_format == kRawRaw12 ? 3 * (x0 >> 1) : x0;
-    tma_load_2d(&map, boxes + b * 64 * 128, &bars[b], bx, ty * 64, static_cast<unsigned int>(kBoxRows * box_bytes));
+    tma_load_2d(&map, boxes + b * 64 * 128, &bars[b], awb_box_x(p.raw_format, x0), ty * 64,
+                static_cast<unsigned int>(kBoxRows * box_bytes));
   };
   if (use_tma && tid == 0 && tile < tiles) issue(tile, 0);
   for (; tile < tiles; tile += gridDim.x) {
@@ -227,33 +92,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
     buf ^= 1;
     ++done;
   }
-  // Flush: block sums, then one atomic per sum and per non-empty bin.
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    u64 v = acc[k];
-#pragma unroll
-    for (int offset = 16; offset > 0; offset >>= 1) v += __shfl_down_sync(0xFFFFFFFFU, v, offset);
-    if ((tid & 31) == 0) red[tid >> 5] = v;
-    __syncthreads();
-    if (tid == 0) {
-      u64 total = 0;
-      for (int w = 0; w < kWarps; ++w) total += red[w];
-      if (total != 0) atomicAdd(k < 3 ? &s->awb_sum[k] : &s->awb_quads, total);
-    }
-    __syncthreads();
-  }
-  if constexpr (kWhitePatch) {
-    for (int i = tid; i < 3 * kAwbBins; i += kThreads) {
-      if (hist[i] != 0U) atomicAdd(&s->awb_hist[0][0] + i, hist[i]);
-    }
-  }
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) last = atomicAdd(&s->awb_done, done) + done == static_cast<unsigned int>(tiles);
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  awb_finish(p, s, red, &first);
+  awb_flush(p, acc, hist, kWhitePatch, red, &first, &last, done, static_cast<unsigned int>(tiles));
 }
 
 template <bool kWhitePatch>

@@ -1,0 +1,251 @@
+// isp_batch.cuh - frames of uneven size, format, Bayer pattern and settings
+// in one launch per pass: the statistics pass over the auto-white-balance
+// frames' tiles, then the tile pass over every frame's tiles.
+//
+// Each pass is a persistent kernel over a work list: CTA i owns the
+// contiguous items ranges[i] (sized by the host so the estimated cost is
+// even), walks them frame by frame, keeps the frame's FrameDesc and tone
+// table in shared memory, prefetches the next item's raw box by TMA
+// (whichever frame it belongs to), and flushes a frame's sums when it leaves
+// it; the CTA that completes a frame's count of tiles finishes that frame
+// (its statistics and histogram, or its white balance estimate). Every tile
+// runs the same device code as the single-frame kernels (isp_main.cuh,
+// isp_awb.cuh), so a frame's bytes are the same alone or in a batch.
+#pragma once
+
+#include "isp_awb.cuh"
+#include "isp_main.cuh"
+
+namespace isp_b200 {
+namespace {
+
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
+// Copies a frame's FrameDesc to shared memory (all threads; the caller syncs).
+__device__ __forceinline__ void load_desc(FrameDesc* dst, const FrameDesc* src) {
+  constexpr int kWords = sizeof(FrameDesc) / 4;
+  static_assert(sizeof(FrameDesc) % 4 == 0, "FrameDesc words");
+  const unsigned int* s = reinterpret_cast<const unsigned int*>(src);
+  unsigned int* d = reinterpret_cast<unsigned int*>(dst);
+  for (int i = threadIdx.x; i < kWords; i += kThreads) d[i] = s[i];
+}
+
+// The frame holding work item `item`, searching forward from frame `from`.
+__device__ __forceinline__ int frame_of_item(const BatchFrame* frames, int nframes, int from, int item, bool awb) {
+  int f = from;
+  while (f + 1 < nframes && item >= (awb ? frames[f + 1].awb_begin : frames[f + 1].tile_begin)) ++f;
+  return f;
+}
+
+template <bool kLutSmem>
+__global__ void __launch_bounds__(kThreads, 2) isp_batch_kernel(const BatchFrame* frames, int nframes,
+                                                                const int2* ranges) {
+  using GS = Geom<true>;  // the sharpening geometry holds every variant's
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
+  const TileSmem m = carve(smem, layout_of(true, box_row_bytes(kRawU16), kLutSmem ? kBatchLutEntries : 0), GS::kSH);
+  __shared__ uint64_t bar;
+  __shared__ u64 red[kWarps];
+  __shared__ int minmax[2];
+  __shared__ bool last;
+  __shared__ __align__(16) FrameDesc fd;
+  const int2 r = ranges[blockIdx.x];
+  if (r.x >= r.y) return;
+  const int tid = threadIdx.x;
+  if (tid == 0) mbar_init(&bar);
+  int f = frame_of_item(frames, nframes, 0, r.x, false);
+  load_desc(&fd, &frames[f].desc);
+  __syncthreads();
+  FrameSetup fs = setup_frame<kLutSmem>(fd, m);
+  __syncthreads();
+
+  const auto issue = [&](int g, int item) {
+    const BatchFrame& bf = frames[g];
+    const int local = item - bf.tile_begin;
+    const int ty = local / bf.tiles_x;
+    const int x0 = (local - ty * bf.tiles_x) * kTW;
+    const int halo = (bf.variant & 2) ? 4 : 2;
+    const int fmt = bf.desc.raw_format;
+    tensormap_acquire(&bf.main_map);
+    tma_load_2d(&bf.main_map, m.box, &bar, box_x(fmt, x0), ty * kTH - halo,
+                static_cast<unsigned int>((kTH + 2 * halo) * box_row_bytes(fmt)));
+  };
+  if (tid == 0 && frames[f].use_tma) issue(f, r.x);
+  uint32_t phase = 0;
+  u64 acc[4] = {0, 0, 0, 0};
+  unsigned int done = 0;
+  for (int item = r.x; item < r.y; ++item) {
+    if (item >= frames[f].tile_begin + frames[f].tiles) {
+      flush_frame(fd, fs, acc, m.hist, red, &last, done, static_cast<unsigned int>(frames[f].tiles));
+      __syncthreads();
+      f = frame_of_item(frames, nframes, f, item, false);
+      load_desc(&fd, &frames[f].desc);
+      __syncthreads();
+      fs = setup_frame<kLutSmem>(fd, m);
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[k] = 0;
+      done = 0;
+    }
+    const BatchFrame& bf = frames[f];
+    const int local = item - bf.tile_begin;
+    const int ty = local / bf.tiles_x;
+    const int x0 = (local - ty * bf.tiles_x) * kTW;
+    const bool use_tma = bf.use_tma != 0;
+    const auto prefetch = [&] {
+      if (tid == 0 && item + 1 < r.y) {
+        const int g = frame_of_item(frames, nframes, f, item + 1, false);
+        if (frames[g].use_tma) {
+          fence_async_shared();
+          issue(g, item + 1);
+        }
+      }
+    };
+    switch (bf.variant) {
+      case 0: run_tile<false, false, 0, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
+      case 1: run_tile<true, false, 0, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
+      case 2: run_tile<false, true, 0, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
+      case 3: run_tile<true, true, 0, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
+      case 4: run_tile<false, false, 1, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
+      case 5: run_tile<true, false, 1, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
+      case 6: run_tile<false, true, 1, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
+      default: run_tile<true, true, 1, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
+    }
+    ++done;
+  }
+  flush_frame(fd, fs, acc, m.hist, red, &last, done, static_cast<unsigned int>(frames[f].tiles));
+}
+
+// The statistics tile of a frame for its Bayer pattern and mode.
+template <int kSrc>
+__device__ __forceinline__ void awb_tile_any(const FrameDesc& p, int pattern, bool white_patch, const uint8_t* box,
+                                             int box_bytes, int x0, int y0, const LscTile& lt, const int* row_k,
+                                             const float* row_ty, const float* table, const float (&black)[4],
+                                             const float (&inv)[4], unsigned int* hist, unsigned int (&sum)[3],
+                                             unsigned int& quads) {
+#define ISP_AWB_CASE(P, W) \
+  awb_tile_fmt<kSrc, W, P>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads)
+  switch (pattern * 2 + (white_patch ? 1 : 0)) {
+    case 0: ISP_AWB_CASE(0, false); break;
+    case 1: ISP_AWB_CASE(0, true); break;
+    case 2: ISP_AWB_CASE(1, false); break;
+    case 3: ISP_AWB_CASE(1, true); break;
+    case 4: ISP_AWB_CASE(2, false); break;
+    case 5: ISP_AWB_CASE(2, true); break;
+    case 6: ISP_AWB_CASE(3, false); break;
+    default: ISP_AWB_CASE(3, true); break;
+  }
+#undef ISP_AWB_CASE
+}
+
+__global__ void __launch_bounds__(kThreads) isp_awb_batch_kernel(const BatchFrame* frames, int nframes,
+                                                               const int2* ranges) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
+  uint8_t* boxes = smem;                                                  // [2][64][128]: double buffer
+  float* table = reinterpret_cast<float*>(smem + 2 * 64 * 128);           // [kLscTableRows][2][kSW]
+  int* col_mx = reinterpret_cast<int*>(table + kLscTableRows * 2 * kSW);  // [64] x 3
+  int* col_ix = col_mx + 64;
+  float* col_tx = reinterpret_cast<float*>(col_ix + 64);
+  int* row_my = reinterpret_cast<int*>(col_tx + 64);                      // [64] x 3
+  int* row_k = row_my + 64;
+  float* row_ty = reinterpret_cast<float*>(row_k + 64);
+  unsigned int* hist = reinterpret_cast<unsigned int*>(row_ty + 64);      // [3][1024]
+  __shared__ uint64_t bars[2];
+  __shared__ u64 red[kWarps];
+  __shared__ int minmax[2];
+  __shared__ int first;
+  __shared__ bool last;
+  __shared__ __align__(16) FrameDesc fd;
+  const int2 r = ranges[blockIdx.x];
+  if (r.x >= r.y) return;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bars[0]);
+    mbar_init(&bars[1]);
+  }
+  for (int i = tid; i < 3 * kAwbBins; i += kThreads) hist[i] = 0U;
+  int f = frame_of_item(frames, nframes, 0, r.x, true);
+  load_desc(&fd, &frames[f].desc);
+  __syncthreads();
+  const auto issue = [&](int g, int item, int b) {
+    const BatchFrame& bf = frames[g];
+    const int local = item - bf.awb_begin;
+    const int ty = local / bf.awb_tiles_x;
+    const int x0 = (local - ty * bf.awb_tiles_x) * 64;
+    const int fmt = bf.desc.raw_format;
+    tensormap_acquire(&bf.awb_map);
+    tma_load_2d(&bf.awb_map, boxes + b * 64 * 128, &bars[b], awb_box_x(fmt, x0), ty * 64,
+                static_cast<unsigned int>(64 * awb_box_bytes(fmt)));
+  };
+  if (tid == 0 && frames[f].use_tma) issue(f, r.x, 0);
+  uint32_t phases = 0;
+  int buf = 0;
+  u64 acc[4] = {0, 0, 0, 0};
+  unsigned int done = 0;
+  for (int item = r.x; item < r.y; ++item) {
+    if (item >= frames[f].awb_begin + frames[f].awb_tiles) {
+      awb_flush(fd, acc, hist, fd.awb_mode == kWbWhitePatch, red, &first, &last, done,
+                static_cast<unsigned int>(frames[f].awb_tiles));
+      f = frame_of_item(frames, nframes, f, item, true);
+      load_desc(&fd, &frames[f].desc);
+      for (int i = tid; i < 3 * kAwbBins; i += kThreads) hist[i] = 0U;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[k] = 0;
+      done = 0;
+      __syncthreads();
+    }
+    const BatchFrame& bf = frames[f];
+    // The other buffer was read by the previous item (the block synchronised
+    // since): load the next item into it while this one is summed.
+    if (tid == 0 && item + 1 < r.y) {
+      const int g = frame_of_item(frames, nframes, f, item + 1, true);
+      if (frames[g].use_tma) {
+        fence_async_shared();
+        issue(g, item + 1, buf ^ 1);
+      }
+    }
+    const int local = item - bf.awb_begin;
+    const int ty = local / bf.awb_tiles_x;
+    const int x0 = (local - ty * bf.awb_tiles_x) * 64;
+    const int y0 = ty * 64;
+    const LscTile lt = build_lsc(fd, fd.pattern, x0, 64, y0, 64, false, 0, 0, col_mx, col_ix, col_tx, row_my, row_k,
+                                 row_ty, table, minmax);
+    const bool use_tma = bf.use_tma != 0;
+    if (use_tma) {
+      if (!mbar_wait(&bars[buf], (phases >> buf) & 1U) && tid == 0) atomicExch(&fd.scratch->error, 1);
+      phases ^= 1U << buf;
+    }
+    float black[4], inv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      black[k] = fd.black[fd.cfa[k]];
+      inv[k] = fd.inv_range[fd.cfa[k]];
+    }
+    unsigned int sum[3] = {0U, 0U, 0U};
+    unsigned int quads = 0;
+    const int box_bytes = awb_box_bytes(fd.raw_format);
+    const bool wp = fd.awb_mode == kWbWhitePatch;
+    if (use_tma) {
+      awb_tile_any<0>(fd, fd.pattern, wp, boxes + buf * 64 * 128, box_bytes, x0, y0, lt, row_k, row_ty, table, black,
+                      inv, hist, sum, quads);
+    } else {
+      awb_tile_any<1>(fd, fd.pattern, wp, boxes + buf * 64 * 128, box_bytes, x0, y0, lt, row_k, row_ty, table, black,
+                      inv, hist, sum, quads);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] += sum[k];
+    acc[3] += quads;
+    __syncthreads();
+    if (use_tma) buf ^= 1;
+    ++done;
+  }
+  awb_flush(fd, acc, hist, fd.awb_mode == kWbWhitePatch, red, &first, &last, done,
+            static_cast<unsigned int>(frames[f].awb_tiles));
+}
+
+}  // namespace
+}  // namespace isp_b200

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <set>
@@ -38,7 +39,7 @@ constexpr int kCfa[4][4] = {
 };
 
 std::mutex g_shapes_mutex;
-std::vector<LaunchShapes> g_shapes;  // per device
+std::deque<LaunchShapes> g_shapes;  // per device; growing keeps references valid
 
 }  // namespace
 
@@ -183,8 +184,6 @@ FrameDesc make_desc(const isp_params_c& p, const DeviceState& s, const isp_raw_v
   return d;
 }
 
-namespace {
-
 LaunchShapes& shapes_for_current_device(cudaError_t* error) {
   int device = 0;
   *error = cudaGetDevice(&device);
@@ -196,8 +195,6 @@ LaunchShapes& shapes_for_current_device(cudaError_t* error) {
   }
   return s;
 }
-
-}  // namespace
 
 namespace {
 
@@ -319,23 +316,6 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
 
 using namespace isp_b200;
 
-struct isp_b200_pipeline {
-  OwnedParams params;
-  DeviceState state;
-  int device = 0;
-  cudaEvent_t done = nullptr;
-  bool queued = false;
-  // Staging for isp_b200_process_host, grown on demand.
-  cudaStream_t host_stream = nullptr;
-  void* d_raw = nullptr;
-  size_t d_raw_cap = 0;
-  void* d_out = nullptr;
-  size_t d_out_cap = 0;
-  void* d_stats = nullptr;  // histogram then statistics
-  // Profiling events around the fused tile kernel (isp_b200_set_kernel_events).
-  cudaEvent_t before_main = nullptr;
-  cudaEvent_t after_main = nullptr;
-};
 
 extern "C" {
 

@@ -87,6 +87,9 @@ constexpr size_t kSmemPerTwoCtas = 112U * 1024U;
 // (and a zeroed map) when the frame's base or pitch is not 16-byte aligned.
 bool encode_raw_map(const FrameDesc& d, int box_row_bytes, int box_rows, CUtensorMap* map);
 
+// The launch shapes of the current device (SM count, occupancy cache).
+LaunchShapes& shapes_for_current_device(cudaError_t* error);
+
 // Queues one frame's kernels on `stream` (no host synchronisation).
 // before_main / after_main (may be null) are recorded around the fused tile kernel.
 // `step` names the call that failed.
@@ -94,3 +97,23 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
                          cudaEvent_t before_main, cudaEvent_t after_main, const char** step);
 
 }  // namespace isp_b200
+
+// One camera's pipeline behind the C ABI (isp_b200_create).
+struct isp_b200_pipeline {
+  isp_b200::OwnedParams params;
+  isp_b200::DeviceState state;
+  int device = 0;
+  cudaEvent_t done = nullptr;
+  bool queued = false;
+  // Staging for isp_b200_process_host, grown on demand.
+  cudaStream_t host_stream = nullptr;
+  void* d_raw = nullptr;
+  size_t d_raw_cap = 0;
+  void* d_out = nullptr;
+  size_t d_out_cap = 0;
+  void* d_stats = nullptr;  // histogram then statistics
+  // Profiling events around the fused tile kernel (isp_b200_set_kernel_events).
+  cudaEvent_t before_main = nullptr;
+  cudaEvent_t after_main = nullptr;
+};
+

@@ -8,6 +8,10 @@ const void* main_kernel_bn(int layout, bool lut_smem);
 const void* main_kernel_bs(int layout, bool lut_smem);
 const void* main_kernel_mn(int layout, bool lut_smem);
 const void* main_kernel_ms(int layout, bool lut_smem);
+const void* batch_kernel_shared_lut();
+const void* batch_kernel_global_lut();
+
+const void* batch_kernel(bool lut_smem) { return lut_smem ? batch_kernel_shared_lut() : batch_kernel_global_lut(); }
 
 const void* main_kernel(bool malvar, bool sharpen, int pattern, bool lut_smem) {
   // RGGB and BGGR share a layout (red/blue on the quad's diagonal), as do

@@ -29,5 +29,15 @@ int awb_kernel_tiles(int width, int height, int* tiles_x);
 
 // Tone tables up to this many entries may be copied into shared memory.
 constexpr int kLutSmemEntries = 4097;
+// In a batch, tone tables up to this many entries go to shared memory.
+constexpr int kBatchLutEntries = 1024;
+
+// The batch passes (isp_batch.cu): arguments (const BatchFrame* frames, int
+// nframes, const int2* ranges), one range of work items per CTA. The tile
+// pass's dynamic shared memory is batch_kernel_smem(); the statistics pass's
+// is awb_kernel_smem().
+const void* batch_kernel(bool lut_smem);
+size_t batch_kernel_smem(bool lut_smem);
+const void* awb_batch_kernel();
 
 }  // namespace isp_b200

@@ -117,10 +117,10 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
   t.table = m.table;
   t.lt = build_lsc(p, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, !interior, p.width + 3, p.height + G::kHalo - 1,
                    m.col_mx, m.col_ix, m.col_tx, m.row_my, m.row_k, m.row_ty, m.table, minmax);
-  if (use_tma && !mbar_wait(bar, phase)) {
-    if (tid == 0) atomicExch(&p.scratch->error, 1);
+  if (use_tma) {
+    if (!mbar_wait(bar, phase) && tid == 0) atomicExch(&p.scratch->error, 1);
+    phase ^= 1U;
   }
-  phase ^= 1U;
 
   // A. Samples of the tile and its halo, preprocessed once.
   unsigned int saturated;

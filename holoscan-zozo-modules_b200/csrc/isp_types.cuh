@@ -1,6 +1,8 @@
 // isp_types.cuh - the device-side descriptors of the B200 ISP.
 #pragma once
 
+#include <cuda.h>
+
 #include <cstdint>
 
 namespace isp_b200 {
@@ -88,6 +90,23 @@ struct FrameDesc {
   int awb_mode;
   float awb_percentile;
   float awb_smoothing;
+};
+
+// One frame of a batch, in device memory: its TMA descriptors, its
+// FrameDesc, and where its tiles sit in the two passes' work lists (items of
+// a frame are consecutive; frames in order).
+struct alignas(64) BatchFrame {
+  CUtensorMap main_map;  // box of the tile pass, when use_tma
+  CUtensorMap awb_map;   // box of the statistics pass, when use_tma
+  FrameDesc desc;
+  int tiles_x;       // tile pass: tiles across
+  int tiles;         // tile pass: tiles of the frame
+  int tile_begin;    // tile pass: first work item
+  int awb_tiles_x;   // statistics pass: tiles across
+  int awb_tiles;     // statistics pass: tiles (0: manual white balance)
+  int awb_begin;     // statistics pass: first work item
+  int variant;       // bit 0 Malvar, bit 1 sharpening, bit 2 GRBG/GBRG layout
+  int use_tma;
 };
 
 }  // namespace isp_b200

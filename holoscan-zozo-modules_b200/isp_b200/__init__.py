@@ -69,6 +69,16 @@ def lib() -> C.CDLL:
         L.isp_b200_set_kernel_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.isp_b200_process_host.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
                                             P(abi.ExposureC)]
+        L.isp_b200_batch_create.argtypes = [C.c_int32, P(C.c_void_p)]
+        L.isp_b200_batch_destroy.argtypes = [C.c_void_p]
+        L.isp_b200_batch_clear.argtypes = [C.c_void_p]
+        L.isp_b200_batch_size.argtypes = [C.c_void_p]
+        L.isp_b200_batch_add.argtypes = [C.c_void_p, C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
+                                         P(abi.ExposureC)]
+        L.isp_b200_batch_launch.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+        L.isp_b200_batch_autotune.argtypes = [C.c_void_p, C.c_void_p]
+        L.isp_b200_batch_set_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+        L.isp_b200_batch_info.argtypes = [C.c_void_p, P(abi.BatchInfoC)]
         if L.isp_b200_abi_version() != abi.ABI_VERSION:
             raise RuntimeError("libisp_b200.so ABI version mismatch")
         _lib = L
@@ -182,6 +192,59 @@ class Pipeline:
         exp = abi.ExposureC(exposure[0], exposure[1])
         check(lib().isp_b200_process_host(self.handle, C.byref(view), C.byref(rgb), C.byref(st), C.byref(exp)))
         return Result(image, hist, stats)
+
+
+class Batch:
+    """Frames of many cameras through one launch per pass (isp_b200_batch_*)."""
+
+    def __init__(self, capacity: int):
+        handle = C.c_void_p()
+        check(lib().isp_b200_batch_create(capacity, C.byref(handle)))
+        self.handle = handle
+        self._keep = []
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().isp_b200_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def clear(self) -> None:
+        check(lib().isp_b200_batch_clear(self.handle))
+        self._keep = []
+
+    def __len__(self) -> int:
+        return int(lib().isp_b200_batch_size(self.handle))
+
+    def add(self, camera: "Pipeline", raw: abi.RawViewC, out: abi.RgbViewC, histogram_ptr: int = 0,
+            stats_ptr: int = 0, exposure: Tuple[int, float] = (0, 0.0)) -> None:
+        st = abi.StatsC(histogram_ptr or None, stats_ptr or None)
+        exp = abi.ExposureC(exposure[0], exposure[1])
+        check(lib().isp_b200_batch_add(self.handle, camera.handle, C.byref(raw), C.byref(out), C.byref(st),
+                                       C.byref(exp)))
+        self._keep.append(camera)
+
+    def launch(self, stream: int = 0, use_graph: bool = False) -> None:
+        check(lib().isp_b200_batch_launch(self.handle, stream or None, 1 if use_graph else 0))
+
+    def autotune(self, stream: int = 0) -> None:
+        check(lib().isp_b200_batch_autotune(self.handle, stream or None))
+
+    def set_tuning(self, weights, ctas_per_sm: int = 0) -> None:
+        w = (C.c_float * 4)(*weights)
+        check(lib().isp_b200_batch_set_tuning(self.handle, w, ctas_per_sm))
+
+    def info(self) -> dict:
+        i = abi.BatchInfoC()
+        check(lib().isp_b200_batch_info(self.handle, C.byref(i)))
+        return {"frames": i.frames, "weights": list(i.weights), "ctas_per_sm": i.ctas_per_sm, "tuned": bool(i.tuned),
+                "graph_replays": i.graph_replays, "graph_main_ctas": i.graph_main_ctas,
+                "graph_awb_ctas": i.graph_awb_ctas}
 
 
 def params_default() -> abi.ParamsC:

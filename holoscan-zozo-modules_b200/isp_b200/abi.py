@@ -98,6 +98,11 @@ class ExposureC(C.Structure):
     _fields_ = [("exposure_ns", C.c_int64), ("gain", C.c_float)]
 
 
+class BatchInfoC(C.Structure):
+    _fields_ = [("frames", C.c_int32), ("weights", C.c_float * 4), ("ctas_per_sm", C.c_int32), ("tuned", C.c_int32),
+                ("graph_replays", C.c_int32), ("graph_main_ctas", C.c_int32), ("graph_awb_ctas", C.c_int32)]
+
+
 @dataclass
 class AutoExposure:
     """AutoExposureParams (isp_params.hpp:82-93), with the reference's defaults."""

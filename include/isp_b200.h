@@ -194,6 +194,48 @@ ISP_B200_API int isp_b200_process_host(isp_b200_pipeline* pipeline, const isp_ra
  * AwbState (isp_math.hpp:71-74). Waits for the queued frames. */
 ISP_B200_API int isp_b200_awb_state(isp_b200_pipeline* pipeline, float gains[3], int32_t* valid);
 
+/* ---- Batches: many cameras' frames, one launch per pass ----------------
+ * No reference counterpart: the reference processes one frame per
+ * IspPipeline::process call. A batch holds frames of different cameras
+ * (pipelines), sizes, formats, Bayer patterns and settings; a launch runs
+ * the white balance statistics of the frames that estimate it, then every
+ * frame's tiles, each pass one persistent kernel over a work list, directly
+ * or as a CUDA graph replayed while the batch keeps its shape (frame count
+ * and work split). Each frame's results are those of isp_b200_process. */
+typedef struct isp_b200_batch isp_b200_batch;
+
+typedef struct isp_batch_info_c {
+  int32_t frames;
+  float weights[4];   /* relative cost of a tile: bilinear, Malvar, +sharpening */
+  int32_t ctas_per_sm; /* 0: as many as fit */
+  int32_t tuned;
+  int32_t graph_replays;
+  int32_t graph_main_ctas;
+  int32_t graph_awb_ctas;
+} isp_batch_info_c;
+
+/* A batch of up to `capacity` frames on the current device. */
+ISP_B200_API int isp_b200_batch_create(int32_t capacity, isp_b200_batch** out);
+ISP_B200_API void isp_b200_batch_destroy(isp_b200_batch* batch);
+/* Forgets the frames (the tuning and the graph stay). */
+ISP_B200_API int isp_b200_batch_clear(isp_b200_batch* batch);
+ISP_B200_API int isp_b200_batch_size(const isp_b200_batch* batch);
+/* Adds a frame of `camera` (device buffers, as isp_b200_process takes them);
+ * a camera appears at most once per batch. ISP_EBUSY when full. */
+ISP_B200_API int isp_b200_batch_add(isp_b200_batch* batch, isp_b200_pipeline* camera, const isp_raw_view_c* raw,
+                       const isp_rgb_view_c* out, const isp_stats_c* stats,
+                       const isp_exposure_c* exposure);
+/* Queues the batch on `stream`; use_graph != 0 replays (or first builds) the
+ * batch's CUDA graph. Each camera's earlier frames run first. */
+ISP_B200_API int isp_b200_batch_launch(isp_b200_batch* batch, void* stream, int32_t use_graph);
+/* Measures the batch's per-variant tile costs and the best CTAs per SM on
+ * this GPU (the frames are processed a few times; the cameras' white balance
+ * states are restored) and keeps them for later launches. */
+ISP_B200_API int isp_b200_batch_autotune(isp_b200_batch* batch, void* stream);
+/* Sets the tuning by hand: weights per variant, CTAs per SM (0: all that fit). */
+ISP_B200_API int isp_b200_batch_set_tuning(isp_b200_batch* batch, const float weights[4], int32_t ctas_per_sm);
+ISP_B200_API int isp_b200_batch_info(const isp_b200_batch* batch, isp_batch_info_c* info);
+
 /* Profiling hook, no reference counterpart: events (cudaEvent_t, may be null)
  * that every following process call records on its stream right before and
  * right after the fused tile kernel, so a caller can time that kernel alone. */
