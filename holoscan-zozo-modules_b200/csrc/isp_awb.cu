@@ -51,8 +51,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   }
   u64 acc[4] = {0, 0, 0, 0};
   uint32_t phases = 0;  // bit b: parity of buffer b's next completion
-  unsigned int done = 0;  // tiles this CTA summed
-  int buf = 0;
+  unsigned int done = 0;  // tiles this CTA summed; its k-th tile uses buffer k & 1
   int tile = blockIdx.x;
   const auto issue = [&](int t, int b) {
     const int ty = t / tiles_x;
@@ -65,6 +64,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
     const int ty = tile / tiles_x;
     const int x0 = (tile - ty * tiles_x) * 64;
     const int y0 = ty * 64;
+    const int buf = static_cast<int>(done & 1U);
     // The other buffer was read by the previous tile (the block synchronised
     // since): load the next tile into it while this one is summed.
     if (use_tma && tid == 0 && tile + static_cast<int>(gridDim.x) < tiles) {
@@ -89,7 +89,6 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
     for (int k = 0; k < 3; ++k) acc[k] += sum[k];
     acc[3] += quads;
     __syncthreads();
-    buf ^= 1;
     ++done;
   }
   awb_flush(p, acc, hist, kWhitePatch, red, &first, &last, done, static_cast<unsigned int>(tiles));

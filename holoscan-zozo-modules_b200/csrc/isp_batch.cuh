@@ -182,8 +182,9 @@ __global__ void __launch_bounds__(kThreads) isp_awb_batch_kernel(const BatchFram
                 static_cast<unsigned int>(64 * awb_box_bytes(fmt)));
   };
   if (tid == 0 && frames[f].use_tma) issue(f, r.x, 0);
-  uint32_t phases = 0;
-  int buf = 0;
+  // Item i of the range uses buffer (i - r.x) & 1, whether or not its frame
+  // uses TMA, so the prefetching thread and the waiting block always agree.
+  uint32_t phases = 0;  // bit b: parity of buffer b's next completion
   u64 acc[4] = {0, 0, 0, 0};
   unsigned int done = 0;
   for (int item = r.x; item < r.y; ++item) {
@@ -199,6 +200,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_batch_kernel(const BatchFram
       __syncthreads();
     }
     const BatchFrame& bf = frames[f];
+    const int buf = (item - r.x) & 1;
     // The other buffer was read by the previous item (the block synchronised
     // since): load the next item into it while this one is summed.
     if (tid == 0 && item + 1 < r.y) {
@@ -240,7 +242,6 @@ __global__ void __launch_bounds__(kThreads) isp_awb_batch_kernel(const BatchFram
     for (int k = 0; k < 3; ++k) acc[k] += sum[k];
     acc[3] += quads;
     __syncthreads();
-    if (use_tma) buf ^= 1;
     ++done;
   }
   awb_flush(fd, acc, hist, fd.awb_mode == kWbWhitePatch, red, &first, &last, done,

@@ -453,6 +453,24 @@ int isp_b200_process(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp
   return ISP_OK;
 }
 
+int isp_b200_device_status(isp_b200_pipeline* pl, int32_t* status) {
+  if (pl == nullptr || status == nullptr) return fail(ISP_EINVAL, "pipeline or status is null");
+  if (pl->queued) {
+    const cudaError_t e = cudaEventSynchronize(pl->done);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaEventSynchronize");
+  }
+  int value = 0;
+  const int zero = 0;
+  PrivateStream ps;
+  ps.copy(&value, &pl->state.scratch->error, sizeof(int), cudaMemcpyDeviceToHost);
+  ps.copy(&pl->state.scratch->error, &zero, sizeof(int), cudaMemcpyHostToDevice);
+  const cudaError_t e = ps.finish();
+  if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyAsync");
+  *status = value;
+  clear_error();
+  return ISP_OK;
+}
+
 int isp_b200_set_kernel_events(isp_b200_pipeline* pl, void* before, void* after) {
   if (pl == nullptr) return fail(ISP_EINVAL, "pipeline is null");
   pl->before_main = static_cast<cudaEvent_t>(before);

@@ -66,6 +66,7 @@ def lib() -> C.CDLL:
         L.isp_b200_awb_state.argtypes = [C.c_void_p, C.c_void_p, P(C.c_int32)]
         L.isp_b200_process.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
                                        P(abi.ExposureC), C.c_void_p]
+        L.isp_b200_device_status.argtypes = [C.c_void_p, P(C.c_int32)]
         L.isp_b200_set_kernel_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.isp_b200_process_host.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
                                             P(abi.ExposureC)]
@@ -165,6 +166,12 @@ class Pipeline:
         valid = C.c_int32()
         check(lib().isp_b200_awb_state(self.handle, gains, C.byref(valid)))
         return np.array(list(gains), np.float32), int(valid.value)
+
+    def device_status(self) -> int:
+        """1 if a kernel gave up a bounded wait on this camera's frames since the last call, else 0."""
+        v = C.c_int32()
+        check(lib().isp_b200_device_status(self.handle, C.byref(v)))
+        return int(v.value)
 
     def set_kernel_events(self, before: int = 0, after: int = 0) -> None:
         """Events (cudaEvent_t handles) recorded around the fused tile kernel of every later frame."""

@@ -236,6 +236,12 @@ ISP_B200_API int isp_b200_batch_autotune(isp_b200_batch* batch, void* stream);
 ISP_B200_API int isp_b200_batch_set_tuning(isp_b200_batch* batch, const float weights[4], int32_t ctas_per_sm);
 ISP_B200_API int isp_b200_batch_info(const isp_b200_batch* batch, isp_batch_info_c* info);
 
+/* Device-side status, no reference counterpart: waits for the pipeline's
+ * queued frames, then reports (and clears) whether a kernel gave up a bounded
+ * wait while processing them (*status 1: that frame's output is not
+ * trustworthy), else 0. */
+ISP_B200_API int isp_b200_device_status(isp_b200_pipeline* pipeline, int32_t* status);
+
 /* Profiling hook, no reference counterpart: events (cudaEvent_t, may be null)
  * that every following process call records on its stream right before and
  * right after the fused tile kernel, so a caller can time that kernel alone. */

@@ -36,6 +36,7 @@ def test_device_matches_reference(name):
         _check(name, f, got, case.expected[f], case.with_stats)
         gains, valid = pipe.awb()
         assert np.array_equal(np.array([*gains.view(np.uint32), valid], np.uint32), case.expected[f]["awb"])
+    assert pipe.device_status() == 0, "a kernel gave up a bounded wait"
     pipe.close()
 
 
