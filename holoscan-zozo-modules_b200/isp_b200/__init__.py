@@ -66,6 +66,8 @@ def lib() -> C.CDLL:
         L.isp_b200_awb_state.argtypes = [C.c_void_p, C.c_void_p, P(C.c_int32)]
         L.isp_b200_process.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
                                        P(abi.ExposureC), C.c_void_p]
+        L.isp_b200_process_noalloc.argtypes = [P(abi.ParamsC), P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
+                                               P(abi.ExposureC), C.c_void_p]
         L.isp_b200_device_status.argtypes = [C.c_void_p, P(C.c_int32)]
         L.isp_b200_set_kernel_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.isp_b200_process_host.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
@@ -252,6 +254,16 @@ class Batch:
         return {"frames": i.frames, "weights": list(i.weights), "ctas_per_sm": i.ctas_per_sm, "tuned": bool(i.tuned),
                 "graph_replays": i.graph_replays, "graph_main_ctas": i.graph_main_ctas,
                 "graph_awb_ctas": i.graph_awb_ctas}
+
+
+def process_noalloc(params: IspParams, raw: abi.RawViewC, out: abi.RgbViewC, histogram_ptr: int = 0,
+                    stats_ptr: int = 0, exposure: Tuple[int, float] = (0, 0.0), stream: int = 0) -> None:
+    """One frame (device buffers) without allocating memory: isp_b200_process_noalloc."""
+    h = params.to_c()
+    st = abi.StatsC(histogram_ptr or None, stats_ptr or None)
+    exp = abi.ExposureC(exposure[0], exposure[1])
+    check(lib().isp_b200_process_noalloc(h.ref(), C.byref(raw), C.byref(out), C.byref(st), C.byref(exp),
+                                         stream or None))
 
 
 def params_default() -> abi.ParamsC:

@@ -236,6 +236,24 @@ ISP_B200_API int isp_b200_batch_autotune(isp_b200_batch* batch, void* stream);
 ISP_B200_API int isp_b200_batch_set_tuning(isp_b200_batch* batch, const float weights[4], int32_t ctas_per_sm);
 ISP_B200_API int isp_b200_batch_info(const isp_b200_batch* batch, isp_batch_info_c* info);
 
+/* One frame without allocating memory. No reference counterpart: for callers
+ * that cannot allocate device memory (cudaMalloc forbidden or unsafe where
+ * they run, e.g. a host that owns every allocation or a real-time loop that
+ * must not touch the allocator). The caller passes raw, out, histogram and
+ * stats in device memory and params on the host; the tone table (at most
+ * 4097 entries), lens shading grid (at most 28544 gains), statistics sums and
+ * white balance state live in one 160 KB device array inside this library,
+ * which every GPU that loads it holds until exit; larger tables are refused
+ * with ISP_EINVAL. The frame is processed as the first frame of a fresh
+ * pipeline (auto white balance: its own estimate, unsmoothed). The first call
+ * on a device, with that device current, looks up the array's address; make
+ * it before any stream capture. Calls share the array: consecutive calls on
+ * one stream are ordered, calls that overlap on the GPU race. No cudaMalloc,
+ * cudaFree or other allocating routine is called. */
+ISP_B200_API int isp_b200_process_noalloc(const isp_params_c* params, const isp_raw_view_c* raw,
+                             const isp_rgb_view_c* out, const isp_stats_c* stats,
+                             const isp_exposure_c* exposure, void* stream);
+
 /* Device-side status, no reference counterpart: waits for the pipeline's
  * queued frames, then reports (and clears) whether a kernel gave up a bounded
  * wait while processing them (*status 1: that frame's output is not
