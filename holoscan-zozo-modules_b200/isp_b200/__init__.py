@@ -82,6 +82,19 @@ def lib() -> C.CDLL:
         L.isp_b200_batch_autotune.argtypes = [C.c_void_p, C.c_void_p]
         L.isp_b200_batch_set_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
         L.isp_b200_batch_info.argtypes = [C.c_void_p, P(abi.BatchInfoC)]
+        L.isp_b200_server_config_default.argtypes = [P(abi.ServerConfigC)]
+        L.isp_b200_server_create.argtypes = [P(abi.ServerConfigC), P(C.c_void_p)]
+        L.isp_b200_server_add_stream.argtypes = [C.c_void_p, P(abi.ParamsC), P(abi.ServerStreamC), P(C.c_int32)]
+        L.isp_b200_server_start.argtypes = [C.c_void_p]
+        L.isp_b200_server_submit.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_int64, P(C.c_uint64)]
+        L.isp_b200_server_poll.argtypes = [C.c_void_p, P(abi.ServerResultC), C.c_int32, P(C.c_int32)]
+        L.isp_b200_server_drain.argtypes = [C.c_void_p, C.c_int64]
+        L.isp_b200_server_stats.argtypes = [C.c_void_p, P(abi.ServerStatsC)]
+        L.isp_b200_server_reset_stats.argtypes = [C.c_void_p]
+        L.isp_b200_server_set_source.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t]
+        L.isp_b200_server_run_poisson.argtypes = [C.c_void_p, P(C.c_double), C.c_double, C.c_uint64]
+        L.isp_b200_server_destroy.argtypes = [C.c_void_p]
         if L.isp_b200_abi_version() != abi.ABI_VERSION:
             raise RuntimeError("libisp_b200.so ABI version mismatch")
         _lib = L
@@ -254,6 +267,77 @@ class Batch:
         return {"frames": i.frames, "weights": list(i.weights), "ctas_per_sm": i.ctas_per_sm, "tuned": bool(i.tuned),
                 "graph_replays": i.graph_replays, "graph_main_ctas": i.graph_main_ctas,
                 "graph_awb_ctas": i.graph_awb_ctas}
+
+
+class Server:
+    """Many camera streams with continuous batching (isp_b200_server_*)."""
+
+    def __init__(self, max_batch: int = 64, max_inflight: int = 2, queue_depth: int = 4, slots_per_stream: int = 2,
+                 memory_budget: int = 8 << 30, use_graph: bool = False):
+        cfg = abi.ServerConfigC()
+        lib().isp_b200_server_config_default(C.byref(cfg))
+        cfg.max_batch, cfg.max_inflight, cfg.queue_depth = max_batch, max_inflight, queue_depth
+        cfg.slots_per_stream, cfg.memory_budget, cfg.use_graph = slots_per_stream, memory_budget, int(use_graph)
+        handle = C.c_void_p()
+        check(lib().isp_b200_server_create(C.byref(cfg), C.byref(handle)))
+        self.handle = handle
+        self._keep = []
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().isp_b200_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_stream(self, params: IspParams, width: int, height: int, fmt: int, bit_depth: int, pattern: int,
+                   out_format: int, with_histogram: bool = True, with_stats: bool = True) -> int:
+        h = params.to_c()
+        shape = abi.ServerStreamC(width, height, fmt, bit_depth, pattern, out_format, int(with_histogram),
+                                  int(with_stats))
+        sid = C.c_int32()
+        check(lib().isp_b200_server_add_stream(self.handle, h.ref(), C.byref(shape), C.byref(sid)))
+        return int(sid.value)
+
+    def start(self) -> None:
+        check(lib().isp_b200_server_start(self.handle))
+
+    def submit(self, stream: int, raw: RawFrame, host_out: Optional[np.ndarray] = None,
+               host_hist: Optional[np.ndarray] = None, host_stats: Optional[np.ndarray] = None,
+               arrival_ns: int = 0) -> int:
+        ticket = C.c_uint64()
+        ptr = lambda a: a.ctypes.data if a is not None else None  # noqa: E731
+        check(lib().isp_b200_server_submit(self.handle, stream, raw.data.ctypes.data, raw.pitch, ptr(host_out),
+                                           ptr(host_hist), ptr(host_stats), arrival_ns, C.byref(ticket)))
+        return int(ticket.value)
+
+    def poll(self, capacity: int = 256):
+        buf = (abi.ServerResultC * capacity)()
+        n = C.c_int32()
+        check(lib().isp_b200_server_poll(self.handle, buf, capacity, C.byref(n)))
+        return [buf[i] for i in range(n.value)]
+
+    def drain(self, timeout_s: float = 60.0) -> None:
+        check(lib().isp_b200_server_drain(self.handle, int(timeout_s * 1e9)))
+
+    def stats(self) -> dict:
+        st = abi.ServerStatsC()
+        check(lib().isp_b200_server_stats(self.handle, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in abi.ServerStatsC._fields_}
+
+    def reset_stats(self) -> None:
+        check(lib().isp_b200_server_reset_stats(self.handle))
+
+    def set_source(self, stream: int, raw: RawFrame) -> None:
+        check(lib().isp_b200_server_set_source(self.handle, stream, raw.data.ctypes.data, raw.pitch))
+
+    def run_poisson(self, fps, seconds: float, seed: int = 1) -> None:
+        arr = (C.c_double * len(fps))(*fps)
+        check(lib().isp_b200_server_run_poisson(self.handle, arr, seconds, seed))
 
 
 def process_noalloc(params: IspParams, raw: abi.RawViewC, out: abi.RgbViewC, histogram_ptr: int = 0,

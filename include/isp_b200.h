@@ -236,6 +236,92 @@ ISP_B200_API int isp_b200_batch_autotune(isp_b200_batch* batch, void* stream);
 ISP_B200_API int isp_b200_batch_set_tuning(isp_b200_batch* batch, const float weights[4], int32_t ctas_per_sm);
 ISP_B200_API int isp_b200_batch_info(const isp_b200_batch* batch, isp_batch_info_c* info);
 
+/* ---- Serving: many camera streams, continuous batching -----------------
+ * No reference counterpart (the reference's operator runs one camera on one
+ * worker). A server keeps each stream's pipeline state on the device, takes
+ * frames as they arrive, admits them against a device-memory budget, and
+ * batches whatever is queued into batch launches (isp_b200_batch_*), up to
+ * max_inflight batches on the GPU while newer arrivals queue for the next.
+ * A frame's latency is its arrival to the completion of its batch. */
+typedef struct isp_b200_server isp_b200_server;
+
+typedef struct isp_server_config_c {
+  int32_t max_batch;        /* frames per batch launch */
+  int32_t max_inflight;     /* batches on the GPU at once, 1..8 */
+  int32_t queue_depth;      /* frames a stream may hold waiting for the GPU */
+  int32_t slots_per_stream; /* device buffers per stream for its frames in flight */
+  int64_t memory_budget;    /* bytes the frames in flight may hold on the device */
+  int32_t use_graph;        /* replay a batch's CUDA graph while its shape repeats */
+} isp_server_config_c;
+
+/* A stream's frame shape and outputs. */
+typedef struct isp_server_stream_c {
+  int32_t width;
+  int32_t height;
+  int32_t format;
+  int32_t bit_depth;
+  int32_t pattern;
+  int32_t out_format;
+  int32_t with_histogram;
+  int32_t with_stats;
+} isp_server_stream_c;
+
+/* A completed frame: its outputs stay in the stream's device slot until the
+ * slot serves a later frame (slots_per_stream frames later). */
+typedef struct isp_server_result_c {
+  uint64_t ticket;
+  int32_t stream;
+  uint64_t frame;      /* sequence number within the stream */
+  int64_t arrival_ns;  /* steady clock */
+  int64_t done_ns;     /* when the GPU finished the frame's batch */
+  const void* image;
+  const uint32_t* histogram;
+  const float* stats;
+} isp_server_result_c;
+
+typedef struct isp_server_stats_c {
+  int64_t submitted;
+  int64_t refused; /* queue full */
+  int64_t admitted;
+  int64_t completed;
+  int64_t batches;
+  int64_t completed_pixels;
+  double mean_batch_frames;
+  double p50_ms;
+  double p99_ms;
+  double p999_ms;
+  double max_ms;
+  double gpix_per_s; /* completed pixels over first arrival to last completion */
+  int32_t error;
+} isp_server_stats_c;
+
+ISP_B200_API void isp_b200_server_config_default(isp_server_config_c* config);
+ISP_B200_API int isp_b200_server_create(const isp_server_config_c* config, isp_b200_server** out);
+/* Adds a camera stream (before start): its pipeline, device slots and pinned staging. */
+ISP_B200_API int isp_b200_server_add_stream(isp_b200_server* server, const isp_params_c* params,
+                               const isp_server_stream_c* shape, int32_t* id);
+ISP_B200_API int isp_b200_server_start(isp_b200_server* server);
+/* A frame of `stream` arrived (host memory, copied to pinned staging before
+ * the call returns; arrival_ns 0 for now). host_out/histogram/stats, when not
+ * null, receive copies of the results. ISP_EBUSY when the stream's queue is full. */
+ISP_B200_API int isp_b200_server_submit(isp_b200_server* server, int32_t stream, const void* host_raw, size_t pitch,
+                           void* host_out, uint32_t* host_histogram, float* host_stats, int64_t arrival_ns,
+                           uint64_t* ticket);
+/* Completed frames since the last poll, oldest first. */
+ISP_B200_API int isp_b200_server_poll(isp_b200_server* server, isp_server_result_c* out, int32_t capacity,
+                         int32_t* count);
+/* Waits until every submitted frame completed; ISP_ETIMEOUT after timeout_ns. */
+ISP_B200_API int isp_b200_server_drain(isp_b200_server* server, int64_t timeout_ns);
+ISP_B200_API int isp_b200_server_stats(isp_b200_server* server, isp_server_stats_c* stats);
+ISP_B200_API int isp_b200_server_reset_stats(isp_b200_server* server);
+/* The frame the synthetic arrival driver submits for `stream` (kept pinned). */
+ISP_B200_API int isp_b200_server_set_source(isp_b200_server* server, int32_t stream, const void* host_raw, size_t pitch);
+/* Synthetic arrivals: each stream's source frame submitted at Poisson times
+ * of rate fps[stream] for `seconds`, from the calling thread. */
+ISP_B200_API int isp_b200_server_run_poisson(isp_b200_server* server, const double* fps, double seconds, uint64_t seed);
+/* Finishes the frames in flight, then frees everything. */
+ISP_B200_API void isp_b200_server_destroy(isp_b200_server* server);
+
 /* One frame without allocating memory. No reference counterpart: for callers
  * that cannot allocate device memory (cudaMalloc forbidden or unsafe where
  * they run, e.g. a host that owns every allocation or a real-time loop that
