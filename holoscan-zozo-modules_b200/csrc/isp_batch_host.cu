@@ -4,7 +4,7 @@
 // batch keeps its shape.
 //
 // A launch writes the frames' descriptors (FrameDesc, TMA maps, work-list
-// positions) and the per-CTA work ranges into one of two pinned staging
+// positions) and the per-CTA work ranges into one of four pinned staging
 // slots, copies them to the device on the launch stream, then runs the
 // statistics pass (when a frame estimates its white balance) and the tile
 // pass. Work ranges are contiguous and of even estimated cost: each tile is
@@ -59,13 +59,17 @@ struct Shape {
 
 }  // namespace
 
+// Pinned descriptor slots: up to this many launches may be queued before
+// a launch waits for the oldest one's descriptors to be consumed.
+constexpr int kStagingSlots = 4;
+
 struct isp_b200_batch {
   int capacity = 0;
   std::vector<Entry> entries;
   BatchFrame* d_frames = nullptr;
   int2* d_ranges = nullptr;
   int max_ctas = 0;
-  Slot slots[2];
+  Slot slots[kStagingSlots];
   int next_slot = 0;
   float weights[4] = {kDefaultWeights[0], kDefaultWeights[1], kDefaultWeights[2], kDefaultWeights[3]};
   int ctas_per_sm = 0;  // 0: as many as fit
@@ -328,6 +332,13 @@ int isp_b200_batch_launch(isp_b200_batch* b, void* stream_ptr, int32_t use_graph
       if (e != cudaSuccess) return fail_cuda(e, "cudaStreamWaitEvent");
     }
   }
+  // The device descriptor buffers are shared by all launches: the previous
+  // launch's kernels finish reading them first (whatever its stream).
+  const Slot& previous = b->slots[(b->next_slot + kStagingSlots - 1) % kStagingSlots];
+  if (previous.pending) {
+    e = cudaStreamWaitEvent(stream, previous.consumed, 0);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaStreamWaitEvent");
+  }
   if (use_graph) {
     if (b->exec == nullptr || !(b->graph_shape == shape)) {
       e = make_graph(b, slot, shape);
@@ -352,7 +363,7 @@ int isp_b200_batch_launch(isp_b200_batch* b, void* stream_ptr, int32_t use_graph
   e = cudaEventRecord(slot.consumed, stream);
   if (e != cudaSuccess) return fail_cuda(e, "cudaEventRecord");
   slot.pending = true;
-  b->next_slot ^= 1;
+  b->next_slot = (b->next_slot + 1) % kStagingSlots;
   for (const Entry& en : b->entries) {
     e = cudaEventRecord(en.camera->done, stream);
     if (e != cudaSuccess) return fail_cuda(e, "cudaEventRecord");

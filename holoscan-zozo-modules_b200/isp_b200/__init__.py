@@ -92,8 +92,10 @@ def lib() -> C.CDLL:
         L.isp_b200_server_drain.argtypes = [C.c_void_p, C.c_int64]
         L.isp_b200_server_stats.argtypes = [C.c_void_p, P(abi.ServerStatsC)]
         L.isp_b200_server_reset_stats.argtypes = [C.c_void_p]
-        L.isp_b200_server_set_source.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t]
+        L.isp_b200_server_submit_device.argtypes = L.isp_b200_server_submit.argtypes
+        L.isp_b200_server_add_source.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t, C.c_int32]
         L.isp_b200_server_run_poisson.argtypes = [C.c_void_p, P(C.c_double), C.c_double, C.c_uint64]
+        L.isp_b200_server_run_closed.argtypes = [C.c_void_p, C.c_double]
         L.isp_b200_server_destroy.argtypes = [C.c_void_p]
         if L.isp_b200_abi_version() != abi.ABI_VERSION:
             raise RuntimeError("libisp_b200.so ABI version mismatch")
@@ -273,11 +275,12 @@ class Server:
     """Many camera streams with continuous batching (isp_b200_server_*)."""
 
     def __init__(self, max_batch: int = 64, max_inflight: int = 2, queue_depth: int = 4, slots_per_stream: int = 2,
-                 memory_budget: int = 8 << 30, use_graph: bool = False):
+                 memory_budget: int = 8 << 30, use_graph: bool = False, per_frame: bool = False):
         cfg = abi.ServerConfigC()
         lib().isp_b200_server_config_default(C.byref(cfg))
         cfg.max_batch, cfg.max_inflight, cfg.queue_depth = max_batch, max_inflight, queue_depth
         cfg.slots_per_stream, cfg.memory_budget, cfg.use_graph = slots_per_stream, memory_budget, int(use_graph)
+        cfg.per_frame = int(per_frame)
         handle = C.c_void_p()
         check(lib().isp_b200_server_create(C.byref(cfg), C.byref(handle)))
         self.handle = handle
@@ -295,10 +298,11 @@ class Server:
             pass
 
     def add_stream(self, params: IspParams, width: int, height: int, fmt: int, bit_depth: int, pattern: int,
-                   out_format: int, with_histogram: bool = True, with_stats: bool = True) -> int:
+                   out_format: int, with_histogram: bool = True, with_stats: bool = True,
+                   copy_back: bool = False) -> int:
         h = params.to_c()
         shape = abi.ServerStreamC(width, height, fmt, bit_depth, pattern, out_format, int(with_histogram),
-                                  int(with_stats))
+                                  int(with_stats), int(copy_back))
         sid = C.c_int32()
         check(lib().isp_b200_server_add_stream(self.handle, h.ref(), C.byref(shape), C.byref(sid)))
         return int(sid.value)
@@ -332,12 +336,25 @@ class Server:
     def reset_stats(self) -> None:
         check(lib().isp_b200_server_reset_stats(self.handle))
 
-    def set_source(self, stream: int, raw: RawFrame) -> None:
-        check(lib().isp_b200_server_set_source(self.handle, stream, raw.data.ctypes.data, raw.pitch))
+    def submit_device(self, stream: int, device_raw: int, pitch: int, host_out: Optional[np.ndarray] = None,
+                      host_hist: Optional[np.ndarray] = None, host_stats: Optional[np.ndarray] = None,
+                      arrival_ns: int = 0) -> int:
+        """A frame already in device memory (read in place until it completes)."""
+        ticket = C.c_uint64()
+        ptr = lambda a: a.ctypes.data if a is not None else None  # noqa: E731
+        check(lib().isp_b200_server_submit_device(self.handle, stream, device_raw, pitch, ptr(host_out),
+                                                  ptr(host_hist), ptr(host_stats), arrival_ns, C.byref(ticket)))
+        return int(ticket.value)
+
+    def add_source(self, stream: int, raw: RawFrame, on_device: bool = False) -> None:
+        check(lib().isp_b200_server_add_source(self.handle, stream, raw.data.ctypes.data, raw.pitch, int(on_device)))
 
     def run_poisson(self, fps, seconds: float, seed: int = 1) -> None:
         arr = (C.c_double * len(fps))(*fps)
         check(lib().isp_b200_server_run_poisson(self.handle, arr, seconds, seed))
+
+    def run_closed(self, seconds: float) -> None:
+        check(lib().isp_b200_server_run_closed(self.handle, seconds))
 
 
 def process_noalloc(params: IspParams, raw: abi.RawViewC, out: abi.RgbViewC, histogram_ptr: int = 0,

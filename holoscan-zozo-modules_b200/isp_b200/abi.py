@@ -105,25 +105,27 @@ class BatchInfoC(C.Structure):
 
 class ServerConfigC(C.Structure):
     _fields_ = [("max_batch", C.c_int32), ("max_inflight", C.c_int32), ("queue_depth", C.c_int32),
-                ("slots_per_stream", C.c_int32), ("memory_budget", C.c_int64), ("use_graph", C.c_int32)]
+                ("slots_per_stream", C.c_int32), ("memory_budget", C.c_int64), ("use_graph", C.c_int32),
+                ("per_frame", C.c_int32)]
 
 
 class ServerStreamC(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("format", C.c_int32), ("bit_depth", C.c_int32),
                 ("pattern", C.c_int32), ("out_format", C.c_int32), ("with_histogram", C.c_int32),
-                ("with_stats", C.c_int32)]
+                ("with_stats", C.c_int32), ("copy_back", C.c_int32)]
 
 
 class ServerResultC(C.Structure):
     _fields_ = [("ticket", C.c_uint64), ("stream", C.c_int32), ("frame", C.c_uint64), ("arrival_ns", C.c_int64),
-                ("done_ns", C.c_int64), ("image", C.c_void_p), ("histogram", C.c_void_p), ("stats", C.c_void_p)]
+                ("launch_ns", C.c_int64), ("done_ns", C.c_int64), ("image", C.c_void_p), ("histogram", C.c_void_p), ("stats", C.c_void_p)]
 
 
 class ServerStatsC(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("refused", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
                 ("batches", C.c_int64), ("completed_pixels", C.c_int64), ("mean_batch_frames", C.c_double),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("p999_ms", C.c_double), ("max_ms", C.c_double),
-                ("gpix_per_s", C.c_double), ("error", C.c_int32)]
+                ("gpix_per_s", C.c_double), ("error", C.c_int32), ("p50_wait_ms", C.c_double),
+                ("p99_wait_ms", C.c_double)]
 
 
 @dataclass

@@ -321,6 +321,23 @@ MIXED_BATCH = [
 ]
 
 
+# Camera streams of the serving workload: (count, width, height, format, bits, black, pattern, fps).
+SERVING_STREAMS = [
+    (16, 640, 480, abi.U8, 8, 16.0, abi.RGGB, 120.0),
+    (24, 1920, 1080, abi.U16, 12, 256.0, abi.GBRG, 60.0),
+    (16, 3840, 2160, abi.RAW10, 10, 64.0, abi.GRBG, 30.0),
+    (8, 4096, 3072, abi.U16, 16, 4096.0, abi.BGGR, 15.0),
+]
+
+
+def serving_streams(seed: int = 4242):
+    """The 64 serving streams: cameras (settings fixed by seed, as
+    mixed_cameras) and their nominal frame rates."""
+    cams = mixed_cameras([t[:7] for t in SERVING_STREAMS], seed)
+    fps = [t[7] for t in SERVING_STREAMS for _ in range(t[0])]
+    return cams, fps
+
+
 def mixed_cameras(shapes=None, seed: int = 2024):
     """Cameras of a mixed workload: per camera a seeded choice of manual, gray
     world or white patch white balance and of bilinear or Malvar-He-Cutler

@@ -252,6 +252,8 @@ typedef struct isp_server_config_c {
   int32_t slots_per_stream; /* device buffers per stream for its frames in flight */
   int64_t memory_budget;    /* bytes the frames in flight may hold on the device */
   int32_t use_graph;        /* replay a batch's CUDA graph while its shape repeats */
+  int32_t per_frame;        /* launch each admitted frame alone (isp_b200_process) instead of
+                               one batch launch: the plain per-frame path, for comparison */
 } isp_server_config_c;
 
 /* A stream's frame shape and outputs. */
@@ -264,6 +266,9 @@ typedef struct isp_server_stream_c {
   int32_t out_format;
   int32_t with_histogram;
   int32_t with_stats;
+  int32_t copy_back; /* frames submitted without host result buffers (the synthetic
+                        drivers') copy image, histogram and statistics back to
+                        pinned host memory the server keeps per device slot */
 } isp_server_stream_c;
 
 /* A completed frame: its outputs stay in the stream's device slot until the
@@ -273,7 +278,8 @@ typedef struct isp_server_result_c {
   int32_t stream;
   uint64_t frame;      /* sequence number within the stream */
   int64_t arrival_ns;  /* steady clock */
-  int64_t done_ns;     /* when the GPU finished the frame's batch */
+  int64_t launch_ns;   /* when the frame's batch was launched */
+  int64_t done_ns;     /* when the server saw the frame's batch complete */
   const void* image;
   const uint32_t* histogram;
   const float* stats;
@@ -293,6 +299,8 @@ typedef struct isp_server_stats_c {
   double max_ms;
   double gpix_per_s; /* completed pixels over first arrival to last completion */
   int32_t error;
+  double p50_wait_ms; /* arrival to the launch of the frame's batch (copy and queueing) */
+  double p99_wait_ms;
 } isp_server_stats_c;
 
 ISP_B200_API void isp_b200_server_config_default(isp_server_config_c* config);
@@ -307,6 +315,12 @@ ISP_B200_API int isp_b200_server_start(isp_b200_server* server);
 ISP_B200_API int isp_b200_server_submit(isp_b200_server* server, int32_t stream, const void* host_raw, size_t pitch,
                            void* host_out, uint32_t* host_histogram, float* host_stats, int64_t arrival_ns,
                            uint64_t* ticket);
+/* A frame of `stream` arrived in device memory (written there by a capture
+ * device, for instance): it is read in place, without a copy, and must stay
+ * unchanged until the frame completes. Otherwise as isp_b200_server_submit. */
+ISP_B200_API int isp_b200_server_submit_device(isp_b200_server* server, int32_t stream, const void* device_raw,
+                                  size_t pitch, void* host_out, uint32_t* host_histogram, float* host_stats,
+                                  int64_t arrival_ns, uint64_t* ticket);
 /* Completed frames since the last poll, oldest first. */
 ISP_B200_API int isp_b200_server_poll(isp_b200_server* server, isp_server_result_c* out, int32_t capacity,
                          int32_t* count);
@@ -314,11 +328,22 @@ ISP_B200_API int isp_b200_server_poll(isp_b200_server* server, isp_server_result
 ISP_B200_API int isp_b200_server_drain(isp_b200_server* server, int64_t timeout_ns);
 ISP_B200_API int isp_b200_server_stats(isp_b200_server* server, isp_server_stats_c* stats);
 ISP_B200_API int isp_b200_server_reset_stats(isp_b200_server* server);
-/* The frame the synthetic arrival driver submits for `stream` (kept pinned). */
-ISP_B200_API int isp_b200_server_set_source(isp_b200_server* server, int32_t stream, const void* host_raw, size_t pitch);
-/* Synthetic arrivals: each stream's source frame submitted at Poisson times
- * of rate fps[stream] for `seconds`, from the calling thread. */
+/* Adds a frame (host memory) to the ring of frames the synthetic arrival
+ * drivers submit for `stream`, in turn; call it before the drivers run. The
+ * server keeps a copy: pinned host memory (submitted like
+ * isp_b200_server_submit frames, copied to the device per frame), or device
+ * memory when on_device is set (submitted like isp_b200_server_submit_device
+ * frames: already in HBM on arrival). A stream's sources are all on the
+ * host or all on the device. */
+ISP_B200_API int isp_b200_server_add_source(isp_b200_server* server, int32_t stream, const void* host_raw, size_t pitch,
+                               int32_t on_device);
+/* Synthetic arrivals: each stream's next source frame submitted at Poisson
+ * times of rate fps[stream] for `seconds`, from the calling thread. An
+ * arrival that finds its stream's queue full is refused (counted). */
 ISP_B200_API int isp_b200_server_run_poisson(isp_b200_server* server, const double* fps, double seconds, uint64_t seed);
+/* Saturation: for `seconds`, every stream's queue is kept full with its next
+ * source frames (closed loop), from the calling thread. */
+ISP_B200_API int isp_b200_server_run_closed(isp_b200_server* server, double seconds);
 /* Finishes the frames in flight, then frees everything. */
 ISP_B200_API void isp_b200_server_destroy(isp_b200_server* server);
 
