@@ -5,7 +5,9 @@
 //
 // A launch writes the frames' descriptors (FrameDesc, TMA maps, work-list
 // positions) and the per-CTA work ranges into one of four pinned staging
-// slots, copies them to the device on the launch stream, then runs the
+// slots, has a staging kernel copy them to the device (SM reads of the
+// pinned slot, so that they never queue behind frame transfers on the copy
+// engines) on the launch stream, then runs the
 // statistics pass (when a frame estimates its white balance) and the tile
 // pass. Work ranges are contiguous and of even estimated cost: each tile is
 // weighted by its variant's measured cost (isp_b200_batch_autotune) or a
@@ -42,6 +44,8 @@ struct Entry {
 struct Slot {
   BatchFrame* frames = nullptr;  // pinned
   int2* ranges = nullptr;        // pinned: tile pass then statistics pass
+  const uint4* frames_dev = nullptr;  // the same memory as the device reads it
+  const uint4* ranges_dev = nullptr;
   cudaEvent_t consumed = nullptr;
   bool pending = false;
 };
@@ -77,8 +81,7 @@ struct isp_b200_batch {
   // The graph of the last shape, its nodes, and the slot its copies read.
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  cudaGraphNode_t copy_frames = nullptr;
-  cudaGraphNode_t copy_ranges = nullptr;
+  cudaGraphNode_t stage = nullptr;
   Shape graph_shape;
   int replays = 0;
 };
@@ -155,14 +158,44 @@ cudaError_t build(isp_b200_batch* b, const Slot& slot, Shape* shape) {
   return cudaSuccess;
 }
 
-// Queues the descriptor copies and the two passes on `stream` (direct launch).
-cudaError_t enqueue(isp_b200_batch* b, const Slot& slot, const Shape& s, cudaStream_t stream) {
-  const size_t frame_bytes = sizeof(BatchFrame) * static_cast<size_t>(s.nframes);
-  cudaError_t e = cudaMemcpyAsync(b->d_frames, slot.frames, frame_bytes, cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess) {
-    e = cudaMemcpyAsync(b->d_ranges, slot.ranges, sizeof(int2) * 2 * static_cast<size_t>(b->max_ctas),
-                        cudaMemcpyHostToDevice, stream);
+// The staging kernel's arguments for a slot (kernel arguments are copied at launch).
+struct StageArgs {
+  const uint4* frames_src;
+  uint4* frames_dst;
+  int frame_words;
+  const uint4* ranges_src;
+  uint4* ranges_dst;
+  int range_words;
+  void* args[6];
+  dim3 grid;
+
+  StageArgs(const isp_b200_batch* b, const Slot& slot, const Shape& s)
+      : frames_src(slot.frames_dev),
+        frames_dst(reinterpret_cast<uint4*>(b->d_frames)),
+        frame_words(static_cast<int>(sizeof(BatchFrame) / sizeof(uint4)) * s.nframes),
+        ranges_src(slot.ranges_dev),
+        ranges_dst(reinterpret_cast<uint4*>(b->d_ranges)),
+        range_words(b->max_ctas),  // 2 x max_ctas int2
+        args{&frames_src, &frames_dst, &frame_words, &ranges_src, &ranges_dst, &range_words},
+        grid((frame_words + range_words + kStageThreads - 1) / kStageThreads) {}
+  StageArgs(const StageArgs&) = delete;
+  StageArgs& operator=(const StageArgs&) = delete;
+
+  cudaKernelNodeParams node() {
+    cudaKernelNodeParams kp{};
+    kp.func = const_cast<void*>(batch_stage_kernel());
+    kp.gridDim = grid;
+    kp.blockDim = dim3(kStageThreads);
+    kp.kernelParams = args;
+    return kp;
   }
+};
+static_assert(sizeof(BatchFrame) % sizeof(uint4) == 0, "descriptors are copied in 16-byte words");
+
+// Queues the descriptor staging and the two passes on `stream` (direct launch).
+cudaError_t enqueue(isp_b200_batch* b, const Slot& slot, const Shape& s, cudaStream_t stream) {
+  StageArgs stage(b, slot, s);
+  cudaError_t e = cudaLaunchKernel(batch_stage_kernel(), stage.grid, dim3(kStageThreads), stage.args, 0, stream);
   if (e != cudaSuccess) return e;
   int nframes = s.nframes;
   const int2* awb_ranges = b->d_ranges + b->max_ctas;
@@ -176,7 +209,7 @@ cudaError_t enqueue(isp_b200_batch* b, const Slot& slot, const Shape& s, cudaStr
                           batch_kernel_smem(s.lut_smem), stream);
 }
 
-// Builds the graph of a shape: two copies, then the passes.
+// Builds the graph of a shape: the descriptor staging, then the passes.
 cudaError_t make_graph(isp_b200_batch* b, const Slot& slot, const Shape& s) {
   if (b->exec != nullptr) cudaGraphExecDestroy(b->exec);
   if (b->graph != nullptr) cudaGraphDestroy(b->graph);
@@ -184,14 +217,10 @@ cudaError_t make_graph(isp_b200_batch* b, const Slot& slot, const Shape& s) {
   b->graph = nullptr;
   cudaError_t e = cudaGraphCreate(&b->graph, 0);
   if (e != cudaSuccess) return e;
-  e = cudaGraphAddMemcpyNode1D(&b->copy_frames, b->graph, nullptr, 0, b->d_frames, slot.frames,
-                               sizeof(BatchFrame) * static_cast<size_t>(s.nframes), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) {
-    e = cudaGraphAddMemcpyNode1D(&b->copy_ranges, b->graph, nullptr, 0, b->d_ranges, slot.ranges,
-                                 sizeof(int2) * 2 * static_cast<size_t>(b->max_ctas), cudaMemcpyHostToDevice);
-  }
+  StageArgs stage(b, slot, s);
+  cudaKernelNodeParams sp = stage.node();
+  e = cudaGraphAddKernelNode(&b->stage, b->graph, nullptr, 0, &sp);
   if (e != cudaSuccess) return e;
-  cudaGraphNode_t copies[2] = {b->copy_frames, b->copy_ranges};
   int nframes = s.nframes;  // kernel node arguments are copied when the node is made
   const int2* awb_ranges = b->d_ranges + b->max_ctas;
   cudaGraphNode_t awb = nullptr;
@@ -203,7 +232,7 @@ cudaError_t make_graph(isp_b200_batch* b, const Slot& slot, const Shape& s) {
     kp.blockDim = dim3(kernel_threads());
     kp.sharedMemBytes = static_cast<unsigned int>(awb_kernel_smem());
     kp.kernelParams = args;
-    e = cudaGraphAddKernelNode(&awb, b->graph, copies, 2, &kp);
+    e = cudaGraphAddKernelNode(&awb, b->graph, &b->stage, 1, &kp);
     if (e != cudaSuccess) return e;
   }
   void* args[] = {&b->d_frames, &nframes, &b->d_ranges};
@@ -217,7 +246,7 @@ cudaError_t make_graph(isp_b200_batch* b, const Slot& slot, const Shape& s) {
   if (awb != nullptr) {
     e = cudaGraphAddKernelNode(&main, b->graph, &awb, 1, &kp);
   } else {
-    e = cudaGraphAddKernelNode(&main, b->graph, copies, 2, &kp);
+    e = cudaGraphAddKernelNode(&main, b->graph, &b->stage, 1, &kp);
   }
   if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
   if (e == cudaSuccess) b->graph_shape = s;
@@ -261,6 +290,11 @@ int isp_b200_batch_create(int32_t capacity, isp_b200_batch** out) {
     if (e == cudaSuccess) e = cudaMallocHost(&s.frames, sizeof(BatchFrame) * static_cast<size_t>(capacity));
     if (e == cudaSuccess) e = cudaMallocHost(&s.ranges, sizeof(int2) * 2 * static_cast<size_t>(b->max_ctas));
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.consumed, cudaEventDisableTiming);
+    void* dev = nullptr;
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(&dev, s.frames, 0);
+    s.frames_dev = static_cast<const uint4*>(dev);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(&dev, s.ranges, 0);
+    s.ranges_dev = static_cast<const uint4*>(dev);
   }
   if (e != cudaSuccess) {
     isp_b200_batch_destroy(b);
@@ -344,15 +378,10 @@ int isp_b200_batch_launch(isp_b200_batch* b, void* stream_ptr, int32_t use_graph
       e = make_graph(b, slot, shape);
       if (e != cudaSuccess) return fail_cuda(e, "batch graph");
     }
-    // The copies read this launch's slot.
-    e = cudaGraphExecMemcpyNodeSetParams1D(b->exec, b->copy_frames, b->d_frames, slot.frames,
-                                           sizeof(BatchFrame) * static_cast<size_t>(shape.nframes),
-                                           cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) {
-      e = cudaGraphExecMemcpyNodeSetParams1D(b->exec, b->copy_ranges, b->d_ranges, slot.ranges,
-                                             sizeof(int2) * 2 * static_cast<size_t>(b->max_ctas),
-                                             cudaMemcpyHostToDevice);
-    }
+    // The staging reads this launch's slot.
+    StageArgs stage(b, slot, shape);
+    cudaKernelNodeParams sp = stage.node();
+    e = cudaGraphExecKernelNodeSetParams(b->exec, b->stage, &sp);
     if (e == cudaSuccess) e = cudaGraphLaunch(b->exec, stream);
     if (e == cudaSuccess) ++b->replays;
   } else {

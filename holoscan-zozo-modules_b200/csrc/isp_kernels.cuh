@@ -39,5 +39,10 @@ constexpr int kBatchLutEntries = 1024;
 const void* batch_kernel(bool lut_smem);
 size_t batch_kernel_smem(bool lut_smem);
 const void* awb_batch_kernel();
+// Descriptor staging (isp_batch.cu): arguments (const uint4* frames_src,
+// uint4* frames_dst, int frame_words, const uint4* ranges_src, uint4*
+// ranges_dst, int range_words), one word per thread.
+const void* batch_stage_kernel();
+constexpr int kStageThreads = 256;
 
 }  // namespace isp_b200

@@ -10,9 +10,9 @@
 //      time the worker saw the event complete;
 //   2. admit: waiting frames, oldest arrival first, take a free slot of their
 //      stream while the bytes of the admitted frames stay within the memory
-//      budget, and their host->device copy is issued at once (two copy
-//      streams: one for frames of at least kLargeCopy bytes, one for smaller
-//      frames, so that a small frame does not queue behind a large one);
+//      budget, and their host->device copy is issued at once, on one of
+//      three copy streams by frame size (below kSmallCopy, below kLargeCopy,
+//      larger), so that a small frame does not queue behind a large one;
 //   3. launch: while fewer than max_inflight batches are on the GPU, the
 //      frames whose copies have completed (at most one per stream, its
 //      oldest) form a batch: one statistics pass and one tile pass over all
@@ -51,8 +51,10 @@ int64_t now_ns() {
       .count();
 }
 
-// Raw frames of at least this many bytes are copied on the large-frame copy stream.
+// Copy lanes by raw frame size: below kSmallCopy, below kLargeCopy, larger.
+constexpr size_t kSmallCopy = size_t{1} << 20;
 constexpr size_t kLargeCopy = size_t{8} << 20;
+constexpr int kCopyLanes = 3;
 
 struct Request {
   uint64_t ticket;
@@ -129,8 +131,7 @@ struct isp_b200_server {
   std::vector<std::unique_ptr<Stream>> streams;
   isp_b200_batch* batch_builder = nullptr;
   cudaStream_t compute = nullptr;
-  cudaStream_t copy_large = nullptr;  // raw frames host -> device
-  cudaStream_t copy_small = nullptr;
+  cudaStream_t copy[kCopyLanes] = {};  // raw frames host -> device, by size
   cudaStream_t readback = nullptr;  // results device -> host, off the compute stream
   std::mutex mutex;                 // everything below
   std::condition_variable wake;
@@ -264,7 +265,7 @@ bool admit(isp_b200_server* sv) {
       a.ready = true;
     } else {
       const size_t bytes = s.raw_row * static_cast<size_t>(s.shape.height);
-      cudaStream_t cs = bytes >= kLargeCopy ? sv->copy_large : sv->copy_small;
+      cudaStream_t cs = sv->copy[bytes < kSmallCopy ? 0 : bytes < kLargeCopy ? 1 : 2];
       cudaError_t e = cudaMemcpy2DAsync(slot.raw, s.raw_pitch, a.req.host_raw, a.req.host_pitch, s.raw_row,
                                         static_cast<size_t>(s.shape.height), cudaMemcpyHostToDevice, cs);
       if (e == cudaSuccess) e = cudaEventRecord(slot.copied, cs);
@@ -517,8 +518,9 @@ int isp_b200_server_create(const isp_server_config_c* config, isp_b200_server** 
   sv->config = *config;
   cudaError_t e = cudaGetDevice(&sv->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sv->compute, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sv->copy_large, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sv->copy_small, cudaStreamNonBlocking);
+  for (cudaStream_t& cs : sv->copy) {
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sv->readback, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     isp_b200_server_destroy(sv);
@@ -786,7 +788,7 @@ void isp_b200_server_destroy(isp_b200_server* sv) {
   }
   sv->wake.notify_all();
   if (sv->worker.joinable()) sv->worker.join();
-  for (cudaStream_t s : {sv->compute, sv->copy_large, sv->copy_small, sv->readback}) {
+  for (cudaStream_t s : {sv->compute, sv->copy[0], sv->copy[1], sv->copy[2], sv->readback}) {
     if (s != nullptr) cudaStreamSynchronize(s);
   }
   for (auto& b : sv->inflight) {
@@ -795,7 +797,7 @@ void isp_b200_server_destroy(isp_b200_server* sv) {
   for (cudaEvent_t ev : sv->spare_events) cudaEventDestroy(ev);
   for (auto& s : sv->streams) release_stream(s.get());
   isp_b200_batch_destroy(sv->batch_builder);
-  for (cudaStream_t s : {sv->compute, sv->copy_large, sv->copy_small, sv->readback}) {
+  for (cudaStream_t s : {sv->compute, sv->copy[0], sv->copy[1], sv->copy[2], sv->readback}) {
     if (s != nullptr) cudaStreamDestroy(s);
   }
   delete sv;
