@@ -68,6 +68,23 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def max_over_ranks(x: float, dist=None, device: str = "cuda") -> float:
+    """The largest of every rank's x (all_reduce MAX; x itself on one rank)."""
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, seconds: float, world: int, dist=None, device: str = "cuda") -> float:
+    """Units all ranks processed over the slowest rank's time. Every rank does
+    the same work (replicas, weak scaling), so the job's units are world x
+    units_per_rank and it ends when its slowest rank does."""
+    return world * units_per_rank / max_over_ranks(seconds, dist, device)
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -327,11 +344,8 @@ def run_b200(args):
         clock_info = clocks.stop()
     elapsed_ms = start.elapsed_time(end)
     kernel_ms = sum(b.elapsed_time(a) for b, a in zip(before, after)) / args.steps
-    t = torch.tensor([elapsed_ms], device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_max = float(t.item())
-    value = world * args.steps * w.pixels / (elapsed_max / 1e3) / 1e9
+    elapsed_max = max_over_ranks(elapsed_ms, dist)
+    value = whole_job_rate(args.steps * w.pixels, elapsed_ms / 1e3, world, dist) / 1e9
 
     # End to end through the host-buffer call, pinned host memory, every step.
     e2e_steps = max(3, min(args.steps, 40))
@@ -346,10 +360,7 @@ def run_b200(args):
     for _ in range(e2e_steps):
         pipe.process_host(host_raw_frame, w.out_format, w.with_stats, (10_000_000, 2.0), out=host_out_typed)
     e2e_s = time.perf_counter() - t0
-    t = torch.tensor([e2e_s], device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps * w.pixels / float(t.item()) / 1e9
+    e2e_value = whole_job_rate(e2e_steps * w.pixels, e2e_s, world, dist) / 1e9
     h2d = abi.raw_row_bytes(w.fmt, w.width) * w.height
     d2h = w.height * out_row + (4096 if w.with_hist else 0) + (48 if w.with_stats else 0)
 
@@ -458,11 +469,8 @@ def run_batch(args):
     p_end.record(stream)
     barrier()
     plain_ms = p_start.elapsed_time(p_end) / plain_steps
-    t = torch.tensor([elapsed_ms], device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_max = float(t.item())
-    value = world * args.steps * total_px / (elapsed_max / 1e3) / 1e9
+    elapsed_max = max_over_ranks(elapsed_ms, dist)
+    value = whole_job_rate(args.steps * total_px, elapsed_ms / 1e3, world, dist) / 1e9
     # End to end: every step copies each frame's raw from pinned host memory,
     # runs the batch, and copies each image, histogram and statistics back.
     host_in = [torch.empty(f[0].numel(), dtype=torch.uint8).pin_memory() for f in frames]
@@ -489,10 +497,7 @@ def run_batch(args):
     for _ in range(e2e_steps):
         e2e_step()
     e2e_s = time.perf_counter() - t0
-    t = torch.tensor([e2e_s], device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps * total_px / float(t.item()) / 1e9
+    e2e_value = whole_job_rate(e2e_steps * total_px, e2e_s, world, dist) / 1e9
     h2d = sum(f[0].numel() for f in frames)
     d2h = sum(f[1].numel() + 4096 + 48 for f in frames)
     cpu = None
@@ -657,16 +662,10 @@ def run_serving(args):
     sat_plain_device = serve(True, True, True, args.aux_seconds)
     sat_plain_host = serve(True, False, True, args.aux_seconds, copy_back=True)
 
-    def max_over_ranks(x: float) -> float:
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # Whole-job throughput: every rank's pixels over the slowest rank's span.
     def job(st):
         span = st["completed_pixels"] / (st["gpix_per_s"] * 1e9) if st["gpix_per_s"] > 0 else float("inf")
-        return world * st["completed_pixels"] / max_over_ranks(span) / 1e9, span
+        return whole_job_rate(st["completed_pixels"], span, world, dist) / 1e9, span
 
     value, span = job(sat_device)
     e2e_value, _ = job(sat_host)
