@@ -36,22 +36,32 @@ __host__ __device__ constexpr int cfa_of(int pattern, int pos) {
   return t[pattern][pos];
 }
 
+// Paired pixels. The tile pass computes two pixels in the two lanes of every
+// f32x2 operation: columns c and c + kHalf of the same row, which have the
+// same Bayer colour and so the same arithmetic. Samples and RGB values live
+// in shared memory as float2 pairs {v(c), v(c + kHalf)}, so that each operand
+// is one aligned 8-byte element and neighbours are neighbouring pairs.
+constexpr int kHalf = 32;
+// Paired sample columns: pair s (0..39) holds tile samples s and s + 32
+// (sample s is image column x0 - 4 + s).
+constexpr int kPW = 40;
+// Paired RGB columns (sharpening): pair q (0..33) holds pixels q - 1 and q + 31.
+constexpr int kCW2 = 34;
+
 template <bool kSharpen>
 struct Geom {
   static constexpr int kHalo = kSharpen ? 4 : 2;  // sample rows above and below the tile
   static constexpr int kSH = kTH + 2 * kHalo;
-  static constexpr int kCW = 68;  // RGB planes: x0 - 1 .. x0 + 64, padded
-  static constexpr int kCH = kTH + 2;
+  static constexpr int kCH = kTH + 2;  // RGB rows: y0 - 1 .. y0 + 64
 };
 
 // ---- Shared memory layout -------------------------------------------------
 
 struct Layout {
   int raw;      // TMA box: box rows x box bytes
-  int samples;  // float [kSH][kSW]
-  int rg;       // float2 [kCH][kCW] (sharpening)
-  int b;        // float [kCH][kCW] (sharpening)
-  int lsc;      // float [kLscTableRows][2][kSW]
+  int samples;  // float2 [kSH][kPW]
+  int r, g, b;  // float2 [kCH][kCW2] each (sharpening)
+  int lsc;      // float2 [kLscTableRows][2][kPW]
   int cols;     // int col_mx[kSW]; int col_ix[kSW]; float col_tx[kSW]
   int rows;     // int row_my[kSH]; int row_k[kSH]; float row_ty[kSH]
   int hist;     // u32 [4][256]
@@ -64,18 +74,19 @@ __host__ __device__ constexpr int align128(int v) { return (v + 127) & ~127; }
 __host__ __device__ constexpr Layout layout_of(bool sharpen, int box_bytes_row, int lut_entries) {
   const int halo = sharpen ? 4 : 2;
   const int sh = kTH + 2 * halo;
+  const int plane = align128((kTH + 2) * kCW2 * 8);
   Layout l{};
   int o = 0;
   l.raw = o;
   o = align128(o + sh * box_bytes_row);
   l.samples = o;
-  o = align128(o + sh * kSW * 4);
-  l.rg = o;
-  if (sharpen) o = align128(o + (kTH + 2) * 68 * 8);
-  l.b = o;
-  if (sharpen) o = align128(o + (kTH + 2) * 68 * 4);
+  o = align128(o + sh * kPW * 8);
+  l.r = o;
+  l.g = o + (sharpen ? plane : 0);
+  l.b = o + (sharpen ? 2 * plane : 0);
+  if (sharpen) o += 3 * plane;
   l.lsc = o;
-  o = align128(o + kLscTableRows * 2 * kSW * 4);
+  o = align128(o + kLscTableRows * 2 * kPW * 8);
   l.cols = o;
   o = align128(o + 3 * kSW * 4);
   l.rows = o;
@@ -206,6 +217,9 @@ struct LscTile {
 
 // Fills the column and row maps (mirrored coordinates, grid cells) and, when
 // it fits, the table. Threads 0..ncols-1 do columns, the next nrows do rows.
+// kPaired: the table holds float2 pairs {T(s), T(s + kHalf)} for s < kPW
+// (the tile pass's paired columns); otherwise one float per column.
+template <bool kPaired = false>
 __device__ LscTile build_lsc(const FrameDesc& p, int pattern, int x_first, int ncols, int y_first, int nrows,
                              bool mirror_xy, int xclamp, int yclamp, int* col_mx, int* col_ix, float* col_tx,
                              int* row_my, int* row_k, float* row_ty, float* table, int* minmax) {
@@ -249,134 +263,32 @@ __device__ LscTile build_lsc(const FrameDesc& p, int pattern, int x_first, int n
   if (lt.rows > kLscTableRows) return lt;
   const int step = p.lsc_channels;
   const int planes = step == 4 ? 2 : 1;
-  for (int e = t; e < lt.rows * planes * ncols; e += kThreads) {
-    const int i = e % ncols;
-    const int kp = e / ncols;
-    const int par = kp % planes;
-    const int k = kp / planes;
+  const auto entry = [&](int k, int par, int i) {
     const int ch = step == 4 ? cfa_of(pattern, (par << 1) | (col_mx[i] & 1)) : 0;
     const float* g = p.lsc + ((lt.iy0 + k) * p.lsc_width + col_ix[i]) * step + ch;
-    table[(k * 2 + par) * kSW + i] = g[0] + (g[step] - g[0]) * col_tx[i];
+    return g[0] + (g[step] - g[0]) * col_tx[i];
+  };
+  if constexpr (kPaired) {
+    float2* table2 = reinterpret_cast<float2*>(table);
+    for (int e = t; e < lt.rows * planes * kPW; e += kThreads) {
+      const int i = e % kPW;
+      const int kp = e / kPW;
+      const int par = kp % planes;
+      const int k = kp / planes;
+      table2[(k * 2 + par) * kPW + i] = make_float2(entry(k, par, i), entry(k, par, i + kHalf));
+    }
+  } else {
+    for (int e = t; e < lt.rows * planes * ncols; e += kThreads) {
+      const int i = e % ncols;
+      const int kp = e / ncols;
+      const int par = kp % planes;
+      const int k = kp / planes;
+      table[(k * 2 + par) * kSW + i] = entry(k, par, i);
+    }
   }
   if (t < nrows) row_k[t] -= lt.iy0;
   __syncthreads();
   return lt;
-}
-
-// ---- Per-pixel tail: colour matrix, statistics, tone, codes ---------------
-
-struct Tone {
-  const float2* table;
-  float scale;  // tone_size - 1
-};
-
-__device__ __forceinline__ float tone_of(const Tone& t, float x) {
-  const float f = fmul(x, t.scale);
-  const float m = magic_trunc(f);
-  const float2 e = t.table[magic_int(m)];
-  return fadd(e.x, fmul(fsub(f, fsub(m, kTwo23)), e.y));
-}
-
-// Stores toned RGB of pixels xb..xb+3 of row y (isp_math.hpp:250-276) and
-// counts their 8-bit codes (isp_math.hpp:279-305) into the block's
-// histogram. `full`: all four pixels are inside the image.
-template <int kOut>
-__device__ __forceinline__ void store_row4(const FrameDesc& p, int xb, int y, const float (&t)[4][3], bool full,
-                                           bool want_hist, unsigned int* hist) {
-  uint8_t* row = p.out + static_cast<int64_t>(y) * p.out_pitch;
-  unsigned int q[4][3];
-  const bool vec = full && p.out_vector;
-  if constexpr (kOut == kOutRgb8 || kOut == kOutRgba8) {
-#pragma unroll
-    for (int dx = 0; dx < 4; ++dx) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) q[dx][k] = magic_int(magic_trunc(fadd(fmul(t[dx][k], 255.0F), 0.5F)));
-    }
-    if constexpr (kOut == kOutRgb8) {
-      if (vec) {
-        unsigned int* o = reinterpret_cast<unsigned int*>(row + 3 * xb);
-        o[0] = q[0][0] | (q[0][1] << 8) | (q[0][2] << 16) | (q[1][0] << 24);
-        o[1] = q[1][1] | (q[1][2] << 8) | (q[2][0] << 16) | (q[2][1] << 24);
-        o[2] = q[2][2] | (q[3][0] << 8) | (q[3][1] << 16) | (q[3][2] << 24);
-      } else {
-#pragma unroll
-        for (int dx = 0; dx < 4; ++dx) {
-          if (!full && xb + dx >= p.width) break;
-#pragma unroll
-          for (int k = 0; k < 3; ++k) row[3 * (xb + dx) + k] = static_cast<uint8_t>(q[dx][k]);
-        }
-      }
-    } else {
-      unsigned int w[4];
-#pragma unroll
-      for (int dx = 0; dx < 4; ++dx) w[dx] = q[dx][0] | (q[dx][1] << 8) | (q[dx][2] << 16) | 0xFF000000U;
-      if (vec) {
-        *reinterpret_cast<uint4*>(row + 4 * xb) = make_uint4(w[0], w[1], w[2], w[3]);
-      } else {
-#pragma unroll
-        for (int dx = 0; dx < 4; ++dx) {
-          if (!full && xb + dx >= p.width) break;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) row[4 * (xb + dx) + k] = static_cast<uint8_t>(w[dx] >> (8 * k));
-        }
-      }
-    }
-  } else if constexpr (kOut == kOutRgb16) {
-    unsigned int v[4][3];
-#pragma unroll
-    for (int dx = 0; dx < 4; ++dx) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        v[dx][k] = magic_int(magic_trunc(fadd(fmul(t[dx][k], 65535.0F), 0.5F)));
-        q[dx][k] = ((v[dx][k] + 128U) * 0xFF01U) >> 24;  // == (v * 255 + 32767) / 65535 for v < 2^16
-      }
-    }
-    if (vec) {
-      uint2* o = reinterpret_cast<uint2*>(row + 6 * xb);
-      o[0] = make_uint2(v[0][0] | (v[0][1] << 16), v[0][2] | (v[1][0] << 16));
-      o[1] = make_uint2(v[1][1] | (v[1][2] << 16), v[2][0] | (v[2][1] << 16));
-      o[2] = make_uint2(v[2][2] | (v[3][0] << 16), v[3][1] | (v[3][2] << 16));
-    } else {
-      uint16_t* o = reinterpret_cast<uint16_t*>(row);
-#pragma unroll
-      for (int dx = 0; dx < 4; ++dx) {
-        if (!full && xb + dx >= p.width) break;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) o[3 * (xb + dx) + k] = static_cast<uint16_t>(v[dx][k]);
-      }
-    }
-  } else {
-#pragma unroll
-    for (int dx = 0; dx < 4; ++dx) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) q[dx][k] = magic_int(magic_trunc(fadd(fmul(clamp01(t[dx][k]), 255.0F), 0.5F)));
-    }
-    if (vec) {
-      float4* o = reinterpret_cast<float4*>(row + 12 * xb);
-      o[0] = make_float4(t[0][0], t[0][1], t[0][2], t[1][0]);
-      o[1] = make_float4(t[1][1], t[1][2], t[2][0], t[2][1]);
-      o[2] = make_float4(t[2][2], t[3][0], t[3][1], t[3][2]);
-    } else {
-      float* o = reinterpret_cast<float*>(row);
-#pragma unroll
-      for (int dx = 0; dx < 4; ++dx) {
-        if (!full && xb + dx >= p.width) break;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) o[3 * (xb + dx) + k] = t[dx][k];
-      }
-    }
-  }
-  if (want_hist) {
-#pragma unroll
-    for (int dx = 0; dx < 4; ++dx) {
-      if (!full && xb + dx >= p.width) break;
-      const unsigned int luma = (2126U * q[dx][0] + 7152U * q[dx][1] + 722U * q[dx][2] + 5000U) / 10000U;
-      atomicAdd(&hist[luma], 1U);
-      atomicAdd(&hist[kHistBins + q[dx][0]], 1U);
-      atomicAdd(&hist[2 * kHistBins + q[dx][1]], 1U);
-      atomicAdd(&hist[3 * kHistBins + q[dx][2]], 1U);
-    }
-  }
 }
 
 __device__ __forceinline__ u64 warp_sum(u64 v) {
@@ -532,17 +444,6 @@ __device__ void finish_stats(const FrameDesc& p, const u64 sum[3], u64 saturated
   out[11] = static_cast<float>(static_cast<double>(saturated) / static_cast<double>(pixels));
 }
 
-template <bool kMalvar, int kPat>
-__device__ __forceinline__ void demosaic_at(const float (&w)[6][8], int dy, int dx, float rgb[3]) {
-  float n[5][5];
-#pragma unroll
-  for (int a = 0; a < 5; ++a) {
-#pragma unroll
-    for (int b = 0; b < 5; ++b) n[a][b] = w[dy + a][dx + b];
-  }
-  demosaic<kMalvar>(n, cfa_of(kPat, (dy << 1) | (dx & 1)), rgb);
-}
-
 // ---- The fused tile pass --------------------------------------------------
 
 // Per-tile state the phases share.
@@ -553,169 +454,9 @@ struct TileCtx {
   const int* row_my;
   const int* row_k;
   const float* row_ty;
-  const float* table;
+  const float2* table;  // paired lens shading table
   LscTile lt;
 };
-
-// A. Samples of the tile and its halo, preprocessed once (preprocess,
-//    isp_math.hpp:151-155), four per unit; returns the saturated count of
-//    the tile's own samples (raw >= white, isp_math.hpp:316).
-template <int kFmt, int kSrc, int kHalo>
-__device__ __forceinline__ unsigned int phase_a(const FrameDesc& p, const TileCtx& t, float* S, int box_bytes,
-                                                const float (&qblack)[4], const float (&qinv)[4],
-                                                const float (&qgain)[4], bool want_stats) {
-  // kSrc: 0 interior tile from the TMA box, 1 edge tile from the box
-  // (mirrored columns), 2 no box (global loads, mirrored).
-  constexpr int kSH = kTH + 2 * kHalo;
-  const unsigned int white = static_cast<unsigned int>(p.white);
-  unsigned int saturated = 0;
-  for (int unit = threadIdx.x; unit < kUnitsRow * kSH; unit += kThreads) {
-    const int j = unit / kUnitsRow;
-    const int u = unit - j * kUnitsRow;
-    const int par = j & 1;  // row parity: y0 - halo is even
-    unsigned int s[4];
-    if constexpr (kSrc == 0) {
-      unpack4(kFmt, t.box + j * box_bytes, u, s);
-    } else if constexpr (kSrc == 1) {
-      const uint8_t* row = t.box + (t.row_my[j] - (t.y0 - kHalo)) * box_bytes;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) s[k] = unpack1(kFmt, row, t.col_mx[4 * u + k], t.x0);
-    } else {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) s[k] = static_cast<unsigned int>(load_raw(p, t.col_mx[4 * u + k], t.row_my[j]));
-    }
-    if (want_stats && j >= kHalo && j < kHalo + kTH && u >= 1 && u <= kTW / 4) {
-      const int y = t.y0 + j - kHalo;
-      const int xs = t.x0 + 4 * (u - 1);
-      if (y < p.height) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) saturated += (xs + k < p.width && s[k] >= white) ? 1U : 0U;
-      }
-    }
-    // The row's two quad positions' constants, selected so they stay in registers.
-    const float bl0 = par ? qblack[2] : qblack[0];
-    const float bl1 = par ? qblack[3] : qblack[1];
-    const float iv0 = par ? qinv[2] : qinv[0];
-    const float iv1 = par ? qinv[3] : qinv[1];
-    const float gn0 = par ? qgain[2] : qgain[0];
-    const float gn1 = par ? qgain[3] : qgain[1];
-    float v[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      // linearize (isp_math.hpp:144-148): max((raw - black) * inv_range, 0).
-      const float x = fmul(fsub(magic_to_float(s[k] | kTwo23Bits), (k & 1) ? bl1 : bl0), (k & 1) ? iv1 : iv0);
-      v[k] = fmaxf(x, 0.0F);
-    }
-    if (t.lt.rows > 0) {
-      if (t.lt.rows <= kLscTableRows) {
-        const int kk = t.row_k[j];
-        const int pl = p.lsc_channels == 4 ? par : 0;
-        const float4 t0 = *reinterpret_cast<const float4*>(t.table + (kk * 2 + pl) * kSW + 4 * u);
-        const float4 t1 = *reinterpret_cast<const float4*>(t.table + ((kk + 1) * 2 + pl) * kSW + 4 * u);
-        const float tyj = t.row_ty[j];
-        v[0] = fmul(v[0], fadd(t0.x, fmul(fsub(t1.x, t0.x), tyj)));
-        v[1] = fmul(v[1], fadd(t0.y, fmul(fsub(t1.y, t0.y), tyj)));
-        v[2] = fmul(v[2], fadd(t0.z, fmul(fsub(t1.z, t0.z), tyj)));
-        v[3] = fmul(v[3], fadd(t0.w, fmul(fsub(t1.w, t0.w), tyj)));
-      } else {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          v[k] = fmul(v[k], lens_shading_gain(p, p.lsc, t.col_mx[4 * u + k], t.row_my[j], p.cfa[(par << 1) | (k & 1)]));
-        }
-      }
-    }
-    // White balance and the clip to 1 (v >= 0): the saturating multiply.
-    *reinterpret_cast<float4*>(S + j * kSW + 4 * u) =
-        make_float4(mul_sat(v[0], gn0), mul_sat(v[1], gn1), mul_sat(v[2], gn0), mul_sat(v[3], gn1));
-  }
-  return saturated;
-}
-
-template <int kSrc, int kHalo>
-__device__ __forceinline__ unsigned int phase_a_fmt(const FrameDesc& p, const TileCtx& t, float* S, int box_bytes,
-                                                    const float (&qblack)[4], const float (&qinv)[4],
-                                                    const float (&qgain)[4], bool want_stats) {
-  // Global loads (no TMA box) read the format at run time in load_raw.
-  if constexpr (kSrc == 2) return phase_a<kRawU8, kSrc, kHalo>(p, t, S, box_bytes, qblack, qinv, qgain, want_stats);
-  switch (p.raw_format) {
-    case kRawU8: return phase_a<kRawU8, kSrc, kHalo>(p, t, S, box_bytes, qblack, qinv, qgain, want_stats);
-    case kRawU16: return phase_a<kRawU16, kSrc, kHalo>(p, t, S, box_bytes, qblack, qinv, qgain, want_stats);
-    case kRawRaw10: return phase_a<kRawRaw10, kSrc, kHalo>(p, t, S, box_bytes, qblack, qinv, qgain, want_stats);
-    default: return phase_a<kRawRaw12, kSrc, kHalo>(p, t, S, box_bytes, qblack, qinv, qgain, want_stats);
-  }
-}
-
-// The tone curve (isp_math.hpp:235-243) from a table of (lut[i], lut[i+1] -
-// lut[i]) pairs: f = x (N - 1), i = trunc(f), lut[i] + (f - i) * diff[i].
-// The last entry's difference is -0.0, so x = 1 (t = +0) returns lut[N-1]
-// exactly, as the reference's branch does, whatever the sign of lut[N-1].
-template <bool kLutSmem>
-__device__ __forceinline__ float tone_at(const float2* table, float scale, float x) {
-  const float f = fmul(x, scale);
-  const float m = magic_trunc(f);
-  float2 e;
-  if constexpr (kLutSmem) {
-    // Shared address of entry trunc(f): base + 8 (bits - 2^23 bits), wrapping.
-    const uint32_t addr = smem_u32(table) + (__float_as_uint(m) << 3) - (kTwo23Bits << 3);
-    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(e.x), "=f"(e.y) : "r"(addr));
-  } else {
-    e = __ldg(table + magic_int(m));
-  }
-  return fadd(e.x, fmul(fsub(f, fsub(m, kTwo23)), e.y));
-}
-
-// C. One 2x4 unit's RGB -> colour matrix, statistics sums, tone, store,
-//    histogram codes. `full`: all eight pixels are inside the image.
-template <int kOut, bool kLutSmem>
-__device__ __forceinline__ void finish_unit(const FrameDesc& p, const float (&rgb)[2][4][3], int xb, int yb,
-                                            bool full, const float2* lut, float lut_scale, bool want_stats,
-                                            bool want_hist, unsigned int* hist, unsigned int (&sums)[3],
-                                            unsigned int& counted) {
-#pragma unroll
-  for (int dy = 0; dy < 2; ++dy) {
-    const int y = yb + dy;
-    if (!full && y >= p.height) continue;
-    float toned[4][3];
-#pragma unroll
-    for (int dx = 0; dx < 4; ++dx) {
-      const float* c = rgb[dy][dx];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        // clamp01((m0 r + m1 g) + m2 b), isp_math.hpp:229-233.
-        const float lin = add_sat(fadd(fmul(p.ccm[3 * k], c[0]), fmul(p.ccm[3 * k + 1], c[1])), fmul(p.ccm[3 * k + 2], c[2]));
-        if (want_stats && (full || xb + dx < p.width)) {
-          // to_fixed (isp_math.hpp:245-247): trunc(lin 2^20 + 0.5).
-          sums[k] += magic_int(magic_trunc(fadd(fmul(lin, kFixedOne), 0.5F)));
-        }
-        toned[dx][k] = tone_at<kLutSmem>(lut, lut_scale, lin);
-      }
-    }
-    store_row4<kOut>(p, xb, y, toned, full || xb + 3 < p.width, want_hist, hist);
-  }
-}
-
-
-// finish_unit for the frame's output format, chosen once per unit.
-template <bool kLutSmem>
-__device__ __forceinline__ void finish_unit_any(const FrameDesc& p, const float (&rgb)[2][4][3], int xb, int yb,
-                                                bool full, const float2* lut, float lut_scale, bool want_stats,
-                                                bool want_hist, unsigned int* hist, unsigned int (&sums)[3],
-                                                unsigned int& counted) {
-  switch (p.out_format) {
-    case kOutRgb8:
-      finish_unit<kOutRgb8, kLutSmem>(p, rgb, xb, yb, full, lut, lut_scale, want_stats, want_hist, hist, sums, counted);
-      break;
-    case kOutRgba8:
-      finish_unit<kOutRgba8, kLutSmem>(p, rgb, xb, yb, full, lut, lut_scale, want_stats, want_hist, hist, sums, counted);
-      break;
-    case kOutRgb16:
-      finish_unit<kOutRgb16, kLutSmem>(p, rgb, xb, yb, full, lut, lut_scale, want_stats, want_hist, hist, sums, counted);
-      break;
-    default:
-      finish_unit<kOutRgb32f, kLutSmem>(p, rgb, xb, yb, full, lut, lut_scale, want_stats, want_hist, hist, sums, counted);
-      break;
-  }
-}
 
 }  // namespace
 }  // namespace isp_b200

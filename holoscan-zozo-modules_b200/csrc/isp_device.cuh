@@ -158,6 +158,78 @@ __device__ __forceinline__ float sharpen_one(float c, float m01, float m21, floa
   return add_sat(c, fmul(amount, fsub(c, blur)));
 }
 
+// ---- The same estimates on two pixels at once (f32x2 lanes) ----------------
+//
+// estimate_rb_site, estimate_g_site and sharpen_one with the operations
+// two-lane ones: each lane sees exactly the scalar function's operations, in
+// the same order (sums left to right as written above). A sum that consumes
+// a product runs per lane (isp_ops.cuh: the assembler may fuse two-lane
+// products into two-lane sums).
+
+template <bool kMalvar>
+__device__ __forceinline__ void estimate_rb_site2(const float2 (&n)[5][5], float2& at_green, float2& diagonal) {
+  if constexpr (!kMalvar) {
+    at_green = mul2(add2(add2(add2(n[1][2], n[3][2]), n[2][1]), n[2][3]), bc2(0.25F));
+    diagonal = mul2(add2(add2(add2(n[1][1], n[1][3]), n[3][1]), n[3][3]), bc2(0.25F));
+  } else {
+    const float2 c = n[2][2];
+    const float2 axial1 = add2(add2(add2(n[1][2], n[3][2]), n[2][1]), n[2][3]);
+    const float2 axial2 = add2(add2(add2(n[0][2], n[4][2]), n[2][0]), n[2][4]);
+    const float2 diagonal1 = add2(add2(add2(n[1][1], n[1][3]), n[3][1]), n[3][3]);
+    at_green = mul_sat2(sub2(exact_scale_add2(axial1, bc2(2.0F), mul2(bc2(4.0F), c)), axial2), bc2(0.125F));
+    // 1.5 axial2 is a rounded product: subtracted per lane (isp_ops.cuh).
+    diagonal = mul_sat2(sub_lanes(exact_scale_add2(diagonal1, bc2(2.0F), mul2(bc2(6.0F), c)), mul2(bc2(1.5F), axial2)),
+                        bc2(0.125F));
+  }
+}
+
+template <bool kMalvar>
+__device__ __forceinline__ void estimate_g_site2(const float2 (&n)[5][5], float2& across, float2& down) {
+  if constexpr (!kMalvar) {
+    across = mul2(add2(n[2][1], n[2][3]), bc2(0.5F));
+    down = mul2(add2(n[1][2], n[3][2]), bc2(0.5F));
+  } else {
+    const float2 c5 = mul2(bc2(5.0F), n[2][2]);
+    const float2 diagonal1 = add2(add2(add2(n[1][1], n[1][3]), n[3][1]), n[3][3]);
+    const float2 horizontal2 = add2(n[2][0], n[2][4]);
+    const float2 vertical2 = add2(n[0][2], n[4][2]);
+    // 0.5 v2 is exact except below the normal range: added per lane all the same.
+    across = mul_sat2(add_lanes(sub2(sub2(exact_scale_add2(add2(n[2][1], n[2][3]), bc2(4.0F), c5), horizontal2), diagonal1),
+                                mul2(bc2(0.5F), vertical2)),
+                      bc2(0.125F));
+    down = mul_sat2(add_lanes(sub2(sub2(exact_scale_add2(add2(n[1][2], n[3][2]), bc2(4.0F), c5), vertical2), diagonal1),
+                              mul2(bc2(0.5F), horizontal2)),
+                    bc2(0.125F));
+  }
+}
+
+// RGB of two pixels whose channel is `channel` (isp_math.hpp:193-214).
+template <bool kMalvar>
+__device__ __forceinline__ void demosaic2(const float2 (&n)[5][5], int channel, float2 rgb[3]) {
+  const float2 c = n[2][2];
+  if (channel == kChR || channel == kChB) {
+    float2 g, d;
+    estimate_rb_site2<kMalvar>(n, g, d);
+    rgb[1] = g;
+    rgb[0] = channel == kChR ? c : d;
+    rgb[2] = channel == kChR ? d : c;
+  } else {
+    float2 across, down;
+    estimate_g_site2<kMalvar>(n, across, down);
+    rgb[1] = c;
+    rgb[0] = channel == kChGr ? across : down;
+    rgb[2] = channel == kChGr ? down : across;
+  }
+}
+
+__device__ __forceinline__ float2 sharpen_one2(float2 c, float2 m01, float2 m21, float2 m10, float2 m12, float2 m00,
+                                               float2 m02, float2 m20, float2 m22, float2 amount) {
+  const float2 axial = add2(add2(add2(m01, m21), m10), m12);
+  const float2 corners = add2(add2(add2(m00, m02), m20), m22);
+  const float2 blur = mul2(add2(exact_scale_add2(axial, bc2(2.0F), mul2(bc2(4.0F), c)), corners), bc2(0.0625F));
+  return add_sat2(c, mul2(amount, sub_lanes(c, blur)));  // blur is a product: per lane
+}
+
 // Colour correction (isp_math.hpp:229-233).
 __device__ __forceinline__ void correct_color(const float* ccm, const float in[3], float out[3]) {
 #pragma unroll

@@ -7,7 +7,7 @@
 // so the instances compile in parallel.
 #pragma once
 
-#include "isp_common.cuh"
+#include "isp_pairs.cuh"
 
 namespace isp_b200 {
 namespace {
@@ -15,10 +15,11 @@ namespace {
 // Shared memory of a CTA, carved from one dynamic allocation.
 struct TileSmem {
   uint8_t* box;
-  float* S;
-  float2* Crg;
-  float* Cb;
-  float* table;
+  float2* P;  // paired samples
+  float2* R;  // paired RGB planes (sharpening)
+  float2* G;
+  float2* B;
+  float2* table;  // paired lens shading table
   int* col_mx;
   int* col_ix;
   float* col_tx;
@@ -32,10 +33,11 @@ struct TileSmem {
 __device__ __forceinline__ TileSmem carve(unsigned char* smem, const Layout& L, int sample_rows) {
   TileSmem m;
   m.box = smem + L.raw;
-  m.S = reinterpret_cast<float*>(smem + L.samples);
-  m.Crg = reinterpret_cast<float2*>(smem + L.rg);
-  m.Cb = reinterpret_cast<float*>(smem + L.b);
-  m.table = reinterpret_cast<float*>(smem + L.lsc);
+  m.P = reinterpret_cast<float2*>(smem + L.samples);
+  m.R = reinterpret_cast<float2*>(smem + L.r);
+  m.G = reinterpret_cast<float2*>(smem + L.g);
+  m.B = reinterpret_cast<float2*>(smem + L.b);
+  m.table = reinterpret_cast<float2*>(smem + L.lsc);
   m.col_mx = reinterpret_cast<int*>(smem + L.cols);
   m.col_ix = m.col_mx + kSW;
   m.col_tx = reinterpret_cast<float*>(m.col_ix + kSW);
@@ -93,6 +95,16 @@ __device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const Tile
   return f;
 }
 
+// Output unit u (0..511) of phase C without sharpening: output row and
+// group of four pairs. Each warp's 32 units share one row parity (the
+// Bayer sites are then compile-time), and lanes 8k .. 8k + 7 one row.
+__device__ __forceinline__ void unit_rc(int u, int& r, int& uc) {
+  const int wk = u >> 5;
+  const int lane = u & 31;
+  r = ((wk >> 1) << 3) + ((lane >> 3) << 1) + (wk & 1);
+  uc = lane & 7;
+}
+
 // One 64x64 tile at (x0, y0). `map` is the frame's TMA descriptor (its box
 // is waited for on `bar`); after phase A, when the box is free again,
 // `after_a()` runs (to prefetch the next tile). Adds the tile's statistics
@@ -115,148 +127,85 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
   t.row_k = m.row_k;
   t.row_ty = m.row_ty;
   t.table = m.table;
-  t.lt = build_lsc(p, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, !interior, p.width + 3, p.height + G::kHalo - 1,
-                   m.col_mx, m.col_ix, m.col_tx, m.row_my, m.row_k, m.row_ty, m.table, minmax);
+  t.lt = build_lsc<true>(p, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, !interior, p.width + 3,
+                         p.height + G::kHalo - 1, m.col_mx, m.col_ix, m.col_tx, m.row_my, m.row_k, m.row_ty,
+                         reinterpret_cast<float*>(m.table), minmax);
   if (use_tma) {
     if (!mbar_wait(bar, phase) && tid == 0) atomicExch(&p.scratch->error, 1);
     phase ^= 1U;
   }
 
-  // A. Samples of the tile and its halo, preprocessed once.
+  // A. Samples of the tile and its halo, preprocessed once, as pairs.
   unsigned int saturated;
   if (!use_tma) {
-    saturated = phase_a_fmt<2, G::kHalo>(p, t, m.S, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
+    saturated = phase_a2_fmt<2, G::kHalo>(p, t, m.P, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
   } else if (interior) {
-    saturated = phase_a_fmt<0, G::kHalo>(p, t, m.S, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
+    saturated = phase_a2_fmt<0, G::kHalo>(p, t, m.P, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
   } else {
-    saturated = phase_a_fmt<1, G::kHalo>(p, t, m.S, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
+    saturated = phase_a2_fmt<1, G::kHalo>(p, t, m.P, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
   }
   acc[3] += saturated;
   __syncthreads();
   after_a();
 
-  // B. (Sharpening) RGB of the tile and a one-pixel ring, 2x4 pixels a
-  //    unit; outside the image these are the reference's virtual pixels
-  //    (cpu_pipeline.cpp:22-46).
+  // B. (Sharpening) RGB of the tile and its ring; BGGR and GBRG write the
+  //    demosaic's red into the blue plane and its blue into the red.
   if constexpr (kSharpen) {
-    constexpr int kUnitsB = 17 * 34;
-    for (int unit = tid; unit < kUnitsB; unit += kThreads) {
-      const int qr = unit / 17;
-      const int qc = unit - qr * 17;
-      float w[6][8];
-#pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        const float4 a = *reinterpret_cast<const float4*>(m.S + (2 * qr + r) * kSW + 4 * qc);
-        const float4 b = *reinterpret_cast<const float4*>(m.S + (2 * qr + r) * kSW + 4 * qc + 4);
-        w[r][0] = a.x; w[r][1] = a.y; w[r][2] = a.z; w[r][3] = a.w;
-        w[r][4] = b.x; w[r][5] = b.y; w[r][6] = b.z; w[r][7] = b.w;
-      }
-      const bool inner = qr >= 1 && qr <= 32 && qc >= 1 && qc <= 15;
-#pragma unroll
-      for (int dy = 0; dy < 2; ++dy) {
-        const int cy = 2 * qr + dy - 1;
-#pragma unroll
-        for (int dx = 0; dx < 4; ++dx) {
-          const int cx = 4 * qc + dx - 1;
-          if (!inner && (cy < 0 || cy >= G::kCH || cx < 0 || cx >= kTW + 2)) continue;
-          float rgb[3];
-          demosaic_at<kMalvar, kPat>(w, dy, dx, rgb);
-          m.Crg[cy * G::kCW + cx] = make_float2(rgb[0], rgb[1]);
-          m.Cb[cy * G::kCW + cx] = rgb[2];
-        }
-      }
-    }
+    phase_b2<kMalvar, kPat>(m.P, f.swap_rb ? m.B : m.R, m.G, f.swap_rb ? m.R : m.B);
     __syncthreads();
   }
 
-  // C. Output units of 2x4 pixels: 32 unit rows x 16 unit columns. A
-  //    tile's statistics sums stay below 2^32 per thread (16 pixels of at
-  //    most 2^20).
+  // C. Two units of four pairs of one row per thread. The statistics sums
+  //    stay below 2^32 per thread and tile (16 pixels of at most 2^20).
   unsigned int sums[3] = {0U, 0U, 0U};
-  unsigned int counted = 0;
-  for (int unit = tid; unit < 512; unit += kThreads) {
-    const int ur = unit >> 4;
-    const int uc = unit & 15;
-    float rgb[2][4][3];
+  unsigned int npix = 0;
+  const float2 amount = bc2(p.sharpen);
+#pragma unroll 1
+  for (int k = 0; k < 2; ++k) {
+    const int unit = tid + k * kThreads;
+    int r, uc;
+    float2 rgb[4][3];
     if constexpr (kSharpen) {
-      // 3x3 neighbourhoods from the RGB planes: window rows 2ur..2ur+3,
-      // columns 4uc..4uc+5 (pixel x0 + 4uc + dx sits at column 4uc + dx + 1).
-      float mm[4][6][3];
+      r = unit >> 3;
+      uc = unit & 7;
+      float2 ch[4];
+      sharpen_row4(m.R, r, uc, amount, ch);
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const float2* rg = m.Crg + (2 * ur + r) * G::kCW + 4 * uc;
-        const float4 a = *reinterpret_cast<const float4*>(rg);
-        const float4 b = *reinterpret_cast<const float4*>(rg + 2);
-        const float4 c = *reinterpret_cast<const float4*>(rg + 4);
-        mm[r][0][0] = a.x; mm[r][0][1] = a.y; mm[r][1][0] = a.z; mm[r][1][1] = a.w;
-        mm[r][2][0] = b.x; mm[r][2][1] = b.y; mm[r][3][0] = b.z; mm[r][3][1] = b.w;
-        mm[r][4][0] = c.x; mm[r][4][1] = c.y; mm[r][5][0] = c.z; mm[r][5][1] = c.w;
-        const float* bp = m.Cb + (2 * ur + r) * G::kCW + 4 * uc;
-        const float4 d = *reinterpret_cast<const float4*>(bp);
-        const float2 e = *reinterpret_cast<const float2*>(bp + 4);
-        mm[r][0][2] = d.x; mm[r][1][2] = d.y; mm[r][2][2] = d.z; mm[r][3][2] = d.w;
-        mm[r][4][2] = e.x; mm[r][5][2] = e.y;
-      }
+      for (int i = 0; i < 4; ++i) rgb[i][0] = ch[i];
+      sharpen_row4(m.G, r, uc, amount, ch);
 #pragma unroll
-      for (int dy = 0; dy < 2; ++dy) {
+      for (int i = 0; i < 4; ++i) rgb[i][1] = ch[i];
+      sharpen_row4(m.B, r, uc, amount, ch);
 #pragma unroll
-        for (int dx = 0; dx < 4; ++dx) {
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            rgb[dy][dx][k] = sharpen_one(mm[dy + 1][dx + 1][k], mm[dy][dx + 1][k], mm[dy + 2][dx + 1][k],
-                                         mm[dy + 1][dx][k], mm[dy + 1][dx + 2][k], mm[dy][dx][k], mm[dy][dx + 2][k],
-                                         mm[dy + 2][dx][k], mm[dy + 2][dx + 2][k], p.sharpen);
-          }
-        }
-      }
+      for (int i = 0; i < 4; ++i) rgb[i][2] = ch[i];
     } else {
-      // Samples rows 2ur .. 2ur + 5 (halo 2), columns 4uc + 2 .. 4uc + 9.
-      float w[6][8];
-#pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        if (!kMalvar && (r == 0 || r == 5)) {
-#pragma unroll
-          for (int c = 0; c < 8; ++c) w[r][c] = 0.0F;
-          continue;
-        }
-        const float* row = m.S + (2 * ur + r) * kSW + 4 * uc;
-        const float4 a = *reinterpret_cast<const float4*>(row);
-        const float4 b = *reinterpret_cast<const float4*>(row + 4);
-        const float4 c = *reinterpret_cast<const float4*>(row + 8);
-        w[r][0] = a.z; w[r][1] = a.w; w[r][2] = b.x; w[r][3] = b.y;
-        w[r][4] = b.z; w[r][5] = b.w; w[r][6] = c.x; w[r][7] = c.y;
+      unit_rc(unit, r, uc);
+      if (r & 1) {
+        demosaic_row4<kMalvar, kPat, 1>(m.P, r, uc, rgb);
+      } else {
+        demosaic_row4<kMalvar, kPat, 0>(m.P, r, uc, rgb);
       }
+      if (f.swap_rb) {
 #pragma unroll
-      for (int dy = 0; dy < 2; ++dy) {
-#pragma unroll
-        for (int dx = 0; dx < 4; ++dx) demosaic_at<kMalvar, kPat>(w, dy, dx, rgb[dy][dx]);
-      }
-    }
-    const int xb = x0 + 4 * uc;
-    const int yb = y0 + 2 * ur;
-    const bool full = xb + 3 < p.width && yb + 1 < p.height;
-    if (f.swap_rb) {
-#pragma unroll
-      for (int dy = 0; dy < 2; ++dy) {
-#pragma unroll
-        for (int dx = 0; dx < 4; ++dx) {
-          const float r = rgb[dy][dx][0];
-          rgb[dy][dx][0] = rgb[dy][dx][2];
-          rgb[dy][dx][2] = r;
+        for (int i = 0; i < 4; ++i) {
+          const float2 red = rgb[i][0];
+          rgb[i][0] = rgb[i][2];
+          rgb[i][2] = red;
         }
       }
     }
-    if (full) {
-      finish_unit_any<kLutSmem>(p, rgb, xb, yb, true, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist, sums,
-                                counted);
-    } else if (xb < p.width && yb < p.height) {
-      finish_unit_any<kLutSmem>(p, rgb, xb, yb, false, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist, sums,
-                                counted);
+    const int x = x0 + 4 * uc;
+    const int y = y0 + r;
+    if (y < p.height) {
+      const int nl = min(max(p.width - x, 0), 4);
+      const int nr = min(max(p.width - x - kHalf, 0), 4);
+      finish_pairs_any<kLutSmem>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist, sums,
+                                 npix);
     }
   }
 #pragma unroll
-  for (int k = 0; k < 3; ++k) acc[k] += sums[k];
-  __syncthreads();  // the next tile overwrites the tables, S and C
+  for (int k = 0; k < 3; ++k) acc[k] += sums[k] - npix * kTwo23Bits;  // mod 2^32: the true sum
+  __syncthreads();  // the next tile overwrites the tables, P and the planes
 }
 
 // The main pass's flush of one frame by one CTA, after it processed
