@@ -95,14 +95,20 @@ __device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const Tile
   return f;
 }
 
-// Output unit u (0..511) of phase C without sharpening: output row and
-// group of four pairs. Each warp's 32 units share one row parity (the
-// Bayer sites are then compile-time), and lanes 8k .. 8k + 7 one row.
-__device__ __forceinline__ void unit_rc(int u, int& r, int& uc) {
-  const int wk = u >> 5;
-  const int lane = u & 31;
-  r = ((wk >> 1) << 3) + ((lane >> 3) << 1) + (wk & 1);
-  uc = lane & 7;
+// Output units u (0..511) of phase C: an output row r and group uc of four
+// pairs. A warp's 32 units are 4 rows x 8 groups, and each quarter-warp
+// (whose 16-byte loads share one pass through the banks) takes groups 0..3
+// or 4..7 of two rows. With sharpening the two rows are r and r + 1: the
+// RGB planes' row stride is an odd number of 16-byte chunks, so they meet
+// different banks. Without sharpening a warp keeps one row parity (the
+// Bayer sites are compile-time) and the rows are r and r + 2, which the
+// sample plane's swizzle (psw) sends to different banks.
+__device__ __forceinline__ void unit_rc(int u, bool same_parity, int& r, int& uc) {
+  const int w = u >> 5;
+  const int l = u & 31;
+  const int ro = ((l >> 2) & 1) + ((l >> 4) << 1);  // 0..3
+  uc = (l & 3) | (((l >> 3) & 1) << 2);
+  r = same_parity ? ((w >> 1) << 3) + 2 * ro + (w & 1) : 4 * w + ro;
 }
 
 // One 64x64 tile at (x0, y0). `map` is the frame's TMA descriptor (its box
@@ -166,8 +172,7 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
     int r, uc;
     float2 rgb[4][3];
     if constexpr (kSharpen) {
-      r = unit >> 3;
-      uc = unit & 7;
+      unit_rc(unit, false, r, uc);
       float2 ch[4];
       sharpen_row4(m.R, r, uc, amount, ch);
 #pragma unroll
@@ -179,7 +184,7 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
 #pragma unroll
       for (int i = 0; i < 4; ++i) rgb[i][2] = ch[i];
     } else {
-      unit_rc(unit, r, uc);
+      unit_rc(unit, true, r, uc);
       if (r & 1) {
         demosaic_row4<kMalvar, kPat, 1>(m.P, r, uc, rgb);
       } else {

@@ -27,6 +27,13 @@ namespace {
 
 constexpr int kUnitsA = kPW / 4;  // phase A units per sample row: 4 pairs each
 
+// Bank spread of the sample plane. Pair s of sample row j sits at
+// j * kPW + (s ^ psw(j)): rows 2k and 2k + 1 keep their order, rows 2k + 2
+// and 2k + 3 swap neighbouring 16-byte chunks, so that a quarter-warp
+// reading four groups of row r and four of row r + 2 (same Bayer parity)
+// meets every bank once. Accesses are whole 16-byte chunks (even s).
+__device__ __forceinline__ int psw(int j) { return ((j >> 1) & 1) << 1; }
+
 __device__ __forceinline__ float4 lds4(const float2* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void sts4(float2* p, float2 a, float2 b) {
   *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
@@ -120,9 +127,10 @@ __device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileC
       }
     }
     // White balance and the clip to 1 (v >= 0): the saturating multiply.
-    float2* dst = P + j * kPW + 4 * u;
-    sts4(dst, mul_sat2(v[0], bc2(gn0)), mul_sat2(v[1], bc2(gn1)));
-    sts4(dst + 2, mul_sat2(v[2], bc2(gn0)), mul_sat2(v[3], bc2(gn1)));
+    float2* dst = P + j * kPW;
+    const int sw = psw(j);
+    sts4(dst + ((4 * u) ^ sw), mul_sat2(v[0], bc2(gn0)), mul_sat2(v[1], bc2(gn1)));
+    sts4(dst + ((4 * u + 2) ^ sw), mul_sat2(v[2], bc2(gn0)), mul_sat2(v[3], bc2(gn1)));
   }
   return saturated;
 }
@@ -161,18 +169,20 @@ __device__ __forceinline__ void phase_b2(const float2* P, float2* R, float2* G, 
     float2 w[6][6] = {};
 #pragma unroll
     for (int a = 0; a < 6; ++a) {
-      const float2* row = P + (2 * ur + 1 + a) * kPW + 2 * uq;  // pair 2uq: w column -1
+      const int j = 2 * ur + 1 + a;
+      const float2* row = P + j * kPW;  // pair 2uq is w column -1
+      const int sw = psw(j);
       const bool edge = a == 0 || a == 5;
       const bool mid = a == 2 || a == 3;
       if (!kMalvar && edge) continue;
-      const float4 m1 = lds4(row + 2), m2 = lds4(row + 4);  // w columns 1..4
+      const float4 m1 = lds4(row + ((2 * uq + 2) ^ sw)), m2 = lds4(row + ((2 * uq + 4) ^ sw));  // w columns 1..4
       w[a][1] = lo2(m1);
       w[a][2] = hi2(m1);
       w[a][3] = lo2(m2);
       w[a][4] = hi2(m2);
       if (kMalvar && mid) {
-        w[a][0] = hi2(lds4(row));
-        w[a][5] = lo2(lds4(row + 6));
+        w[a][0] = hi2(lds4(row + ((2 * uq) ^ sw)));
+        w[a][5] = lo2(lds4(row + ((2 * uq + 6) ^ sw)));
       }
     }
     float2 rgb[2][2][3];
@@ -230,17 +240,20 @@ __device__ __forceinline__ void demosaic_row4(const float2* P, int r, int uc, fl
   float2 w[5][8] = {};
 #pragma unroll
   for (int a = 0; a < 5; ++a) {
-    const float2* row = P + (r + a) * kPW + 4 * uc + 2;
+    const float2* row = P + (r + a) * kPW;
+    const int sw = psw(r + a);
+    const int s0 = 4 * uc + 2;
     const bool edge = a == 0 || a == 4;
     if (edge && !kMalvar) continue;
     if (edge) {  // Malvar's vertical taps: the centres only
-      const float4 v1 = lds4(row + 2), v2 = lds4(row + 4);
+      const float4 v1 = lds4(row + ((s0 + 2) ^ sw)), v2 = lds4(row + ((s0 + 4) ^ sw));
       w[a][2] = lo2(v1);
       w[a][3] = hi2(v1);
       w[a][4] = lo2(v2);
       w[a][5] = hi2(v2);
     } else {
-      const float4 v0 = lds4(row), v1 = lds4(row + 2), v2 = lds4(row + 4), v3 = lds4(row + 6);
+      const float4 v0 = lds4(row + (s0 ^ sw)), v1 = lds4(row + ((s0 + 2) ^ sw)), v2 = lds4(row + ((s0 + 4) ^ sw)),
+                   v3 = lds4(row + ((s0 + 6) ^ sw));
       w[a][0] = lo2(v0);
       w[a][1] = hi2(v0);
       w[a][2] = lo2(v1);
