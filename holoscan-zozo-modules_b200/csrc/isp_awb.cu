@@ -13,7 +13,7 @@ namespace {
 // ---- White balance statistics ----------------------------------------------
 
 template <bool kWhitePatch, int kPat>
-__global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant__ CUtensorMap map, FrameDesc p,
+__global__ void __launch_bounds__(kThreads, 3) isp_awb_kernel(const __grid_constant__ CUtensorMap map, FrameDesc p,
                                                          int tiles_x, int tiles, int use_tma) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
@@ -27,6 +27,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   int* row_k = row_my + 64;
   float* row_ty = reinterpret_cast<float*>(row_k + 64);
   unsigned int* hist = reinterpret_cast<unsigned int*>(row_ty + 64);      // [3][1024]
+  float* grid_s = reinterpret_cast<float*>(hist + 3 * kAwbBins);          // [kGridSmemGains]
   __shared__ uint64_t bars[2];
   __shared__ u64 red[kWarps];
   __shared__ int minmax[2];
@@ -37,6 +38,13 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
   const int box_bytes = awb_box_bytes(p.raw_format);
   if constexpr (kWhitePatch) {
     for (int i = tid; i < 3 * kAwbBins; i += kThreads) hist[i] = 0U;
+  }
+  // The lens shading gains in shared memory for the frame, when they fit.
+  const float* grid = p.lsc;
+  const int gains = p.lsc_width * p.lsc_height * p.lsc_channels;
+  if (p.lsc != nullptr && gains <= kGridSmemGains) {
+    for (int i = tid; i < gains; i += kThreads) grid_s[i] = p.lsc[i];
+    grid = grid_s;
   }
   if (tid == 0 && use_tma) {
     mbar_init(&bars[0]);
@@ -71,7 +79,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_kernel(const __grid_constant
       fence_async_shared();
       issue(tile + gridDim.x, buf ^ 1);
     }
-    const LscTile lt = build_lsc(p, kPat, x0, 64, y0, 64, false, 0, 0, col_mx, col_ix, col_tx, row_my, row_k,
+    const LscTile lt = build_lsc(p, grid, kPat, x0, 64, y0, 64, false, 0, 0, col_mx, col_ix, col_tx, row_my, row_k,
                                  row_ty, table, minmax);
     if (use_tma && !mbar_wait(&bars[buf], (phases >> buf) & 1U)) {
       if (tid == 0) atomicExch(&s->error, 1);

@@ -141,7 +141,7 @@ __device__ __forceinline__ void awb_tile_any(const FrameDesc& p, int pattern, bo
 #undef ISP_AWB_CASE
 }
 
-__global__ void __launch_bounds__(kThreads) isp_awb_batch_kernel(const BatchFrame* frames, int nframes,
+__global__ void __launch_bounds__(kThreads, 3) isp_awb_batch_kernel(const BatchFrame* frames, int nframes,
                                                                const int2* ranges) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kThreads) isp_awb_batch_kernel(const BatchFram
     const int ty = local / bf.awb_tiles_x;
     const int x0 = (local - ty * bf.awb_tiles_x) * 64;
     const int y0 = ty * 64;
-    const LscTile lt = build_lsc(fd, fd.pattern, x0, 64, y0, 64, false, 0, 0, col_mx, col_ix, col_tx, row_my, row_k,
+    const LscTile lt = build_lsc(fd, fd.lsc, fd.pattern, x0, 64, y0, 64, false, 0, 0, col_mx, col_ix, col_tx, row_my, row_k,
                                  row_ty, table, minmax);
     const bool use_tma = bf.use_tma != 0;
     if (use_tma) {

@@ -27,14 +27,31 @@ constexpr unsigned int kWaitLimit = 1U << 22;  // bounded mbarrier polls
 // each gain from the grid directly.
 constexpr int kLscTableRows = 8;
 
-// The channel (kChR, kChGr, kChGb, kChB) at quad position (y & 1) * 2 + (x & 1).
-__host__ __device__ constexpr int cfa_of(int pattern, int pos) {
+// The channel (kChR, kChGr, kChGb, kChB) at quad position (y & 1) * 2 + (x & 1)
+// of each Bayer pattern, packed two bits per entry so that a run-time lookup
+// is a shift (a constant array indexed at run time would live in local memory).
+__host__ __device__ constexpr unsigned int cfa_word() {
   constexpr int t[4][4] = {{kChR, kChGr, kChGb, kChB},
                            {kChB, kChGb, kChGr, kChR},
                            {kChGr, kChR, kChB, kChGb},
                            {kChGb, kChB, kChR, kChGr}};
-  return t[pattern][pos];
+  unsigned int w = 0;
+  for (int p = 0; p < 4; ++p) {
+    for (int q = 0; q < 4; ++q) w |= static_cast<unsigned int>(t[p][q]) << (8 * p + 2 * q);
+  }
+  return w;
 }
+constexpr unsigned int kCfaWord = cfa_word();
+__host__ __device__ constexpr int cfa_of(int pattern, int pos) {
+  return static_cast<int>((kCfaWord >> (8 * pattern + 2 * pos)) & 3U);
+}
+static_assert(cfa_of(0, 0) == kChR && cfa_of(1, 3) == kChR && cfa_of(2, 1) == kChR && cfa_of(3, 2) == kChR &&
+                  cfa_of(2, 0) == kChGr && cfa_of(3, 1) == kChB && cfa_of(1, 1) == kChGb,
+              "Bayer channel table");
+
+// Lens shading grids of at most this many gains are kept in shared memory
+// for the frame (a 17 x 13 x 4 grid is 884).
+constexpr int kGridSmemGains = 1024;
 
 // Paired pixels. The tile pass computes two pixels in the two lanes of every
 // f32x2 operation: columns c and c + kHalf of the same row, which have the
@@ -65,6 +82,7 @@ struct Layout {
   int cols;     // int col_mx[kSW]; int col_ix[kSW]; float col_tx[kSW]
   int rows;     // int row_my[kSH]; int row_k[kSH]; float row_ty[kSH]
   int hist;     // u32 [4][256]
+  int grid;     // float [kGridSmemGains]: the frame's lens shading grid, when it fits
   int lut;      // float2 [tone_size] when in shared memory
   int total;
 };
@@ -93,6 +111,8 @@ __host__ __device__ constexpr Layout layout_of(bool sharpen, int box_bytes_row, 
   o = align128(o + 3 * sh * 4);
   l.hist = o;
   o = align128(o + kHistChannels * kHistBins * 4);
+  l.grid = o;
+  o = align128(o + kGridSmemGains * 4);
   l.lut = o;
   o = align128(o + lut_entries * 8);
   l.total = o;
@@ -219,8 +239,11 @@ struct LscTile {
 // it fits, the table. Threads 0..ncols-1 do columns, the next nrows do rows.
 // kPaired: the table holds float2 pairs {T(s), T(s + kHalf)} for s < kPW
 // (the tile pass's paired columns); otherwise one float per column.
+// `grid`: the frame's lens shading gains (the frame's own, or a copy in
+// shared memory).
 template <bool kPaired = false>
-__device__ LscTile build_lsc(const FrameDesc& p, int pattern, int x_first, int ncols, int y_first, int nrows,
+__device__ LscTile build_lsc(const FrameDesc& p, const float* grid, int pattern, int x_first, int ncols, int y_first,
+                             int nrows,
                              bool mirror_xy, int xclamp, int yclamp, int* col_mx, int* col_ix, float* col_tx,
                              int* row_my, int* row_k, float* row_ty, float* table, int* minmax) {
   const int t = threadIdx.x;
@@ -228,6 +251,8 @@ __device__ LscTile build_lsc(const FrameDesc& p, int pattern, int x_first, int n
     minmax[0] = 0x7FFFFFFF;
     minmax[1] = -1;
   }
+  int iy_lo = 0x7FFFFFFF;  // this thread's row's grid row, if it has one
+  int iy_hi = -1;
   __syncthreads();
   if (t < ncols) {
     int x = x_first + t;
@@ -251,8 +276,18 @@ __device__ LscTile build_lsc(const FrameDesc& p, int pattern, int x_first, int n
       iy = iy > p.lsc_height - 2 ? p.lsc_height - 2 : iy;
       row_k[j] = iy;
       row_ty[j] = fy - static_cast<float>(iy);
-      atomicMin(&minmax[0], iy);
-      atomicMax(&minmax[1], iy);
+      iy_lo = iy;
+      iy_hi = iy;
+    }
+  }
+  // The rows' grid range: a warp reduction, then one shared atomic per warp
+  // (same-address shared atomics from every row thread would serialise).
+  if (p.lsc != nullptr) {
+    iy_lo = __reduce_min_sync(0xFFFFFFFFU, iy_lo);
+    iy_hi = __reduce_max_sync(0xFFFFFFFFU, iy_hi);
+    if ((t & 31) == 0 && iy_hi >= 0) {
+      atomicMin(&minmax[0], iy_lo);
+      atomicMax(&minmax[1], iy_hi);
     }
   }
   __syncthreads();
@@ -265,7 +300,7 @@ __device__ LscTile build_lsc(const FrameDesc& p, int pattern, int x_first, int n
   const int planes = step == 4 ? 2 : 1;
   const auto entry = [&](int k, int par, int i) {
     const int ch = step == 4 ? cfa_of(pattern, (par << 1) | (col_mx[i] & 1)) : 0;
-    const float* g = p.lsc + ((lt.iy0 + k) * p.lsc_width + col_ix[i]) * step + ch;
+    const float* g = grid + ((lt.iy0 + k) * p.lsc_width + col_ix[i]) * step + ch;
     return g[0] + (g[step] - g[0]) * col_tx[i];
   };
   if constexpr (kPaired) {
@@ -455,6 +490,7 @@ struct TileCtx {
   const int* row_k;
   const float* row_ty;
   const float2* table;  // paired lens shading table
+  const float* grid;     // the frame's lens shading gains
   LscTile lt;
 };
 

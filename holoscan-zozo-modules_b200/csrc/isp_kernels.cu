@@ -36,8 +36,10 @@ int main_kernel_tiles(int width, int height, int* tiles_x) {
 int kernel_threads() { return kThreads; }
 
 size_t awb_kernel_smem() {
-  // two boxes of 64 x 128, lens shading table, column and row maps, white-patch histogram.
-  return 2U * 64U * 128U + kLscTableRows * 2U * kSW * 4U + 6U * 64U * 4U + 3U * kAwbBins * 4U + 128U;
+  // two boxes of 64 x 128, lens shading table, column and row maps, white-patch
+  // histogram, the frame's lens shading grid.
+  return 2U * 64U * 128U + kLscTableRows * 2U * kSW * 4U + 6U * 64U * 4U + 3U * kAwbBins * 4U + kGridSmemGains * 4U +
+         128U;
 }
 
 int awb_box_row_bytes(int raw_format) {

@@ -27,6 +27,7 @@ struct TileSmem {
   int* row_k;
   float* row_ty;
   unsigned int* hist;
+  float* grid;
   float2* lut_s;
 };
 
@@ -45,6 +46,7 @@ __device__ __forceinline__ TileSmem carve(unsigned char* smem, const Layout& L, 
   m.row_k = m.row_my + sample_rows;
   m.row_ty = reinterpret_cast<float*>(m.row_k + sample_rows);
   m.hist = reinterpret_cast<unsigned int*>(smem + L.hist);
+  m.grid = reinterpret_cast<float*>(smem + L.grid);
   m.lut_s = reinterpret_cast<float2*>(smem + L.lut);
   return m;
 }
@@ -56,6 +58,7 @@ struct FrameSetup {
   float qinv[4];
   float qgain[4];
   const float2* lut;
+  const float* grid;  // lens shading gains: shared memory when they fit
   float lut_scale;
   bool swap_rb;
   bool want_hist;
@@ -76,6 +79,12 @@ __device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const Tile
     f.qblack[k] = p.black[ch];
     f.qinv[k] = p.inv_range[ch];
     f.qgain[k] = f.gains[color_of(ch)];
+  }
+  f.grid = p.lsc;
+  const int gains = p.lsc_width * p.lsc_height * p.lsc_channels;
+  if (p.lsc != nullptr && gains <= kGridSmemGains) {
+    for (int i = threadIdx.x; i < gains; i += kThreads) m.grid[i] = p.lsc[i];
+    f.grid = m.grid;
   }
   f.lut = p.tone;
   if constexpr (kLutSmem) {
@@ -133,7 +142,8 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
   t.row_k = m.row_k;
   t.row_ty = m.row_ty;
   t.table = m.table;
-  t.lt = build_lsc<true>(p, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, !interior, p.width + 3,
+  t.grid = f.grid;
+  t.lt = build_lsc<true>(p, f.grid, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, !interior, p.width + 3,
                          p.height + G::kHalo - 1, m.col_mx, m.col_ix, m.col_tx, m.row_my, m.row_k, m.row_ty,
                          reinterpret_cast<float*>(m.table), minmax);
   if (use_tma) {

@@ -121,8 +121,8 @@ __device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileC
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           const int ch = p.cfa[(par << 1) | (k & 1)];
-          v[k].x = fmul(v[k].x, lens_shading_gain(p, p.lsc, t.col_mx[4 * u + k], t.row_my[j], ch));
-          v[k].y = fmul(v[k].y, lens_shading_gain(p, p.lsc, t.col_mx[4 * u + kHalf + k], t.row_my[j], ch));
+          v[k].x = fmul(v[k].x, lens_shading_gain(p, t.grid, t.col_mx[4 * u + k], t.row_my[j], ch));
+          v[k].y = fmul(v[k].y, lens_shading_gain(p, t.grid, t.col_mx[4 * u + kHalf + k], t.row_my[j], ch));
         }
       }
     }
