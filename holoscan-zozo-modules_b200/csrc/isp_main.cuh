@@ -214,8 +214,13 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
     if (y < p.height) {
       const int nl = min(max(p.width - x, 0), 4);
       const int nr = min(max(p.width - x - kHalf, 0), 4);
-      finish_pairs_any<kLutSmem>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist, sums,
-                                 npix);
+      if (nl == 4 && nr == 4 && p.out_vector) {
+        finish_pairs_any<kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist,
+                                         sums, npix);
+      } else {
+        finish_pairs_any<kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist,
+                                          sums, npix);
+      }
     }
   }
 #pragma unroll

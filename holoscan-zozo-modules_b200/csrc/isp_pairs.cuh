@@ -405,13 +405,17 @@ __device__ __forceinline__ void store_seg4(const FrameDesc& p, int x, int y, con
 // The per-pixel tail of four pairs of one row (pixels x .. x + 3 and
 // x + 32 .. x + 35 of image row y): colour matrix, statistics sums, tone,
 // codes, stores. nl, nr: pixels of the left and right groups inside the
-// image (0..4). sums: 2^23 bits + to_fixed summed mod 2^32, npix the number
-// of terms, so that the caller subtracts npix x 2^23 bits.
-template <int kOut, bool kLutSmem>
-__device__ __forceinline__ void finish_pairs(const FrameDesc& p, const float2 (&rgb)[4][3], int x, int y, int nl,
-                                             int nr, const float2* lut, float lut_scale, bool want_stats,
+// image (0..4); kFull: both are 4 and the rows may be stored 16 bytes at a
+// time (the interior units, compiled without the per-pixel guards). sums:
+// 2^23 bits + to_fixed summed mod 2^32, npix the number of terms, so that the
+// caller subtracts npix x 2^23 bits.
+template <int kOut, bool kLutSmem, bool kFull>
+__device__ __forceinline__ void finish_pairs(const FrameDesc& p, const float2 (&rgb)[4][3], int x, int y, int nl_,
+                                             int nr_, const float2* lut, float lut_scale, bool want_stats,
                                              bool want_hist, unsigned int* hist, unsigned int (&sums)[3],
                                              unsigned int& npix) {
+  const int nl = kFull ? 4 : nl_;
+  const int nr = kFull ? 4 : nr_;
   float tl[4][3], tr[4][3];
   unsigned int cl[4][3], cr[4][3];
 #pragma unroll
@@ -452,27 +456,27 @@ __device__ __forceinline__ void finish_pairs(const FrameDesc& p, const float2 (&
     }
   }
   if (want_stats) npix += static_cast<unsigned int>(nl + nr);
-  if (nl > 0) store_seg4<kOut>(p, x, y, tl, cl, nl, want_hist, hist);
-  if (nr > 0) store_seg4<kOut>(p, x + kHalf, y, tr, cr, nr, want_hist, hist);
+  if (kFull || nl > 0) store_seg4<kOut>(p, x, y, tl, cl, nl, want_hist, hist);
+  if (kFull || nr > 0) store_seg4<kOut>(p, x + kHalf, y, tr, cr, nr, want_hist, hist);
 }
 
-template <bool kLutSmem>
+template <bool kLutSmem, bool kFull>
 __device__ __forceinline__ void finish_pairs_any(const FrameDesc& p, const float2 (&rgb)[4][3], int x, int y, int nl,
                                                  int nr, const float2* lut, float lut_scale, bool want_stats,
                                                  bool want_hist, unsigned int* hist, unsigned int (&sums)[3],
                                                  unsigned int& npix) {
   switch (p.out_format) {
     case kOutRgb8:
-      finish_pairs<kOutRgb8, kLutSmem>(p, rgb, x, y, nl, nr, lut, lut_scale, want_stats, want_hist, hist, sums, npix);
+      finish_pairs<kOutRgb8, kLutSmem, kFull>(p, rgb, x, y, nl, nr, lut, lut_scale, want_stats, want_hist, hist, sums, npix);
       break;
     case kOutRgba8:
-      finish_pairs<kOutRgba8, kLutSmem>(p, rgb, x, y, nl, nr, lut, lut_scale, want_stats, want_hist, hist, sums, npix);
+      finish_pairs<kOutRgba8, kLutSmem, kFull>(p, rgb, x, y, nl, nr, lut, lut_scale, want_stats, want_hist, hist, sums, npix);
       break;
     case kOutRgb16:
-      finish_pairs<kOutRgb16, kLutSmem>(p, rgb, x, y, nl, nr, lut, lut_scale, want_stats, want_hist, hist, sums, npix);
+      finish_pairs<kOutRgb16, kLutSmem, kFull>(p, rgb, x, y, nl, nr, lut, lut_scale, want_stats, want_hist, hist, sums, npix);
       break;
     default:
-      finish_pairs<kOutRgb32f, kLutSmem>(p, rgb, x, y, nl, nr, lut, lut_scale, want_stats, want_hist, hist, sums, npix);
+      finish_pairs<kOutRgb32f, kLutSmem, kFull>(p, rgb, x, y, nl, nr, lut, lut_scale, want_stats, want_hist, hist, sums, npix);
       break;
   }
 }
