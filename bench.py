@@ -268,7 +268,11 @@ def workload_config(w: scene.Workload, nbuf: int = 0):
            "white_balance": ["manual", "gray-world", "white-patch"][w.params.white_balance],
            "demosaic": ["bilinear", "malvar"][w.params.demosaic], "sharpen": w.params.sharpen,
            "histogram": w.with_hist, "stats": w.with_stats, "compulsory_bytes_per_frame": w.compulsory_bytes()}
-    if nbuf:
+    if w.fresh_frames:
+        cfg["frames"] = (f"{w.fresh_frames} fresh-seed frames rendered on the device (isp_b200_synthetic_raw), "
+                         f"taken in turn: {w.fresh_frames * abi.raw_row_bytes(w.fmt, w.width) * w.height / 1e9:.1f} GB "
+                         "of raw, far above the 126 MB L2")
+    elif nbuf:
         cfg["l2"] = f"{nbuf} rotating buffer sets, {nbuf * w.compulsory_bytes() / 1e6:.0f} MB > 126 MB L2"
     return cfg
 
@@ -299,16 +303,29 @@ def run_b200(args):
     raw = w.raw(1 + rank)
     out_row = w.width * abi.output_channels(w.out_format) * abi.output_channel_bytes(w.out_format)
     nbuf = max(2, math.ceil(2 * L2_BYTES / w.compulsory_bytes()))
-    raws = [torch.from_numpy(raw.data).cuda() for _ in range(nbuf)]
+    if w.fresh_frames:
+        # Fresh seeds: distinct frames rendered on the device, taken in turn.
+        nraw = w.fresh_frames
+        raws = []
+        for i in range(nraw):
+            buf = torch.empty(raw.pitch * w.height, dtype=torch.uint8, device="cuda")
+            isp_b200.synthetic_raw(w.width, w.height, w.fmt, w.bits, w.pattern, w.black, 100_000 * (rank + 1) + i,
+                                   buf.data_ptr(), raw.pitch)
+            raws.append(buf)
+        torch.cuda.synchronize()
+    else:
+        nraw = nbuf
+        raws = [torch.from_numpy(raw.data).cuda() for _ in range(nbuf)]
     outs = [torch.empty(w.height * out_row, dtype=torch.uint8, device="cuda") for _ in range(nbuf)]
     hists = [torch.empty(1024, dtype=torch.int32, device="cuda") for _ in range(nbuf)]
     stats = [torch.empty(12, dtype=torch.float32, device="cuda") for _ in range(nbuf)]
     pipe = isp_b200.Pipeline(w.params)
     views = []
-    for i in range(nbuf):
-        rv = abi.RawViewC(raws[i].data_ptr(), w.width, w.height, raw.pitch, w.fmt, w.bits, w.pattern)
-        ov = abi.RgbViewC(outs[i].data_ptr(), out_row, w.out_format)
-        st = abi.StatsC(hists[i].data_ptr() if w.with_hist else None, stats[i].data_ptr() if w.with_stats else None)
+    for i in range(max(nraw, nbuf)):
+        rv = abi.RawViewC(raws[i % nraw].data_ptr(), w.width, w.height, raw.pitch, w.fmt, w.bits, w.pattern)
+        ov = abi.RgbViewC(outs[i % nbuf].data_ptr(), out_row, w.out_format)
+        st = abi.StatsC(hists[i % nbuf].data_ptr() if w.with_hist else None,
+                        stats[i % nbuf].data_ptr() if w.with_stats else None)
         views.append((rv, ov, st))
     exp = abi.ExposureC(10_000_000, 2.0)
     L = isp_b200.lib()
@@ -316,7 +333,7 @@ def run_b200(args):
     sptr = C.c_void_p(stream.cuda_stream)
 
     def step(i):
-        rv, ov, st = views[i % nbuf]
+        rv, ov, st = views[i % len(views)]
         isp_b200.check(L.isp_b200_process(pipe.handle, C.byref(rv), C.byref(ov), C.byref(st), C.byref(exp), sptr))
 
     launches_per_step = 2 if w.params.white_balance != abi.MANUAL else 1
@@ -423,9 +440,7 @@ def run_batch(args):
     pipes = [isp_b200.Pipeline(c.params) for c in cams]
     frames = []
     for i, c in enumerate(cams):
-        counts = scene.device_counts(c.width, c.height, c.pattern, c.black, c.bits, 7000 * (rank + 1) + i)
-        data, row = scene.device_pack(counts, c.fmt)
-        del counts
+        data, row = device_frame(c, 7000 * (rank + 1) + i)
         out_row = c.width * 3
         out = torch.empty(c.height * out_row, dtype=torch.uint8, device="cuda")
         hist = torch.empty(1024, dtype=torch.int32, device="cuda")
@@ -532,6 +547,19 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
+def device_frame(c, seed: int):
+    """Camera c's frame of `seed`, rendered on the device by isp_b200_synthetic_raw:
+    a uint8 tensor of rows and the row bytes."""
+    import torch
+
+    import isp_b200
+
+    row = abi.raw_row_bytes(c.fmt, c.width)
+    data = torch.empty(row * c.height, dtype=torch.uint8, device="cuda")
+    isp_b200.synthetic_raw(c.width, c.height, c.fmt, c.bits, c.pattern, c.black, seed, data.data_ptr(), row)
+    return data, row
+
+
 def cpu_mixed_baseline(cams, picks, seconds: float):
     """The reference CPU backend on one frame of each camera shape in `picks`,
     round robin over all host threads, for about `seconds`."""
@@ -539,9 +567,8 @@ def cpu_mixed_baseline(cams, picks, seconds: float):
     raws = []
     for i in picks:
         c = cams[i]
-        counts = scene.device_counts(c.width, c.height, c.pattern, c.black, c.bits, 99).cpu().numpy()
-        data, pitch = scene.pack(counts.astype(np.uint16), c.fmt)
-        raws.append((c, abi.RawFrame(data, c.width, c.height, pitch, c.fmt, c.bits, c.pattern)))
+        data, pitch = device_frame(c, 99)
+        raws.append((c, abi.RawFrame(data.cpu().numpy(), c.width, c.height, pitch, c.fmt, c.bits, c.pattern)))
     threads = cpu_threads()
     px = 0
     t0 = time.perf_counter()
@@ -600,11 +627,9 @@ def run_serving(args):
     for i, c in enumerate(cams):
         ring = []
         for k in range(n_sources):
-            counts = scene.device_counts(c.width, c.height, c.pattern, c.black, c.bits,
-                                         100_000 * (rank + 1) + 10 * i + k)
-            data, row = scene.device_pack(counts, c.fmt)
+            data, row = device_frame(c, 100_000 * (rank + 1) + 10 * i + k)
             ring.append(abi.RawFrame(data.cpu().numpy(), c.width, c.height, row, c.fmt, c.bits, c.pattern))
-            del counts, data
+            del data
         sources.append(ring)
     torch.cuda.synchronize()
     budget = 8 << 30

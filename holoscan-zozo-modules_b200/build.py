@@ -27,7 +27,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC
           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-DISP_B200_BUILD"]
 
 SOURCES = ["isp_batch.cu", "isp_batch_global_lut.cu", "isp_main_bilinear.cu", "isp_main_bilinear_sharpen.cu", "isp_main_malvar.cu", "isp_main_malvar_sharpen.cu",
-           "isp_awb.cu", "isp_kernels.cu", "isp_capi.cu", "isp_batch_host.cu", "isp_noalloc.cu", "isp_server.cu", "isp_params.cpp"]
+           "isp_awb.cu", "isp_kernels.cu", "isp_capi.cu", "isp_batch_host.cu", "isp_noalloc.cu", "isp_server.cu", "isp_synth.cu", "isp_params.cpp"]
 
 
 def _compile(src: str, verbose: bool) -> str:

@@ -96,6 +96,9 @@ def lib() -> C.CDLL:
         L.isp_b200_server_add_source.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t, C.c_int32]
         L.isp_b200_server_run_poisson.argtypes = [C.c_void_p, P(C.c_double), C.c_double, C.c_uint64]
         L.isp_b200_server_run_closed.argtypes = [C.c_void_p, C.c_double]
+        L.isp_b200_synth_default.argtypes = [P(abi.SynthC)]
+        L.isp_b200_synth_default.restype = None
+        L.isp_b200_synthetic_raw.argtypes = [P(abi.SynthC), C.c_uint64, C.c_void_p, C.c_size_t, C.c_void_p]
         L.isp_b200_server_destroy.argtypes = [C.c_void_p]
         if L.isp_b200_abi_version() != abi.ABI_VERSION:
             raise RuntimeError("libisp_b200.so ABI version mismatch")
@@ -355,6 +358,17 @@ class Server:
 
     def run_closed(self, seconds: float) -> None:
         check(lib().isp_b200_server_run_closed(self.handle, seconds))
+
+
+def synthetic_raw(width: int, height: int, fmt: int, bit_depth: int, pattern: int, black: float, seed: int,
+                  device_raw: int, pitch: int, stream: int = 0, gain: float = 0.5, read_noise: float = 3.0,
+                  vignette_edge: float = 0.5) -> None:
+    """Renders the seeded synthetic frame into device memory (isp_b200_synthetic_raw)."""
+    cfg = abi.SynthC()
+    lib().isp_b200_synth_default(C.byref(cfg))
+    cfg.width, cfg.height, cfg.format, cfg.bit_depth, cfg.pattern = width, height, fmt, bit_depth, pattern
+    cfg.black, cfg.gain, cfg.read_noise, cfg.vignette_edge = black, gain, read_noise, vignette_edge
+    check(lib().isp_b200_synthetic_raw(C.byref(cfg), seed & 0xFFFFFFFFFFFFFFFF, device_raw, pitch, stream or None))
 
 
 def process_noalloc(params: IspParams, raw: abi.RawViewC, out: abi.RgbViewC, histogram_ptr: int = 0,

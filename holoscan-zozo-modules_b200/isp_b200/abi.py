@@ -120,6 +120,12 @@ class ServerResultC(C.Structure):
                 ("launch_ns", C.c_int64), ("done_ns", C.c_int64), ("image", C.c_void_p), ("histogram", C.c_void_p), ("stats", C.c_void_p)]
 
 
+class SynthC(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("format", C.c_int32), ("bit_depth", C.c_int32),
+                ("pattern", C.c_int32), ("black", C.c_float), ("gain", C.c_float), ("read_noise", C.c_float),
+                ("vignette_edge", C.c_float)]
+
+
 class ServerStatsC(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("refused", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
                 ("batches", C.c_int64), ("completed_pixels", C.c_int64), ("mean_batch_frames", C.c_double),

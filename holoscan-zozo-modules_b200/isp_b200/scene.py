@@ -168,6 +168,7 @@ class Workload:
     out_format: int
     with_stats: bool
     with_hist: bool
+    fresh_frames: int = 0  # > 0: the benchmark takes this many distinct frames in turn (device-rendered)
 
     def raw(self, seed: int, pitch: Optional[int] = None, noise: bool = True) -> abi.RawFrame:
         counts = mosaic_counts(self.width, self.height, self.pattern, self.black, (1 << self.bits) - 1,
@@ -212,86 +213,9 @@ def config2(width=8192, height=6144) -> Workload:
                       white_balance=abi.WHITE_PATCH, white_patch_percentile=0.995, demosaic=abi.MALVAR,
                       ccm=CCM, tone_curve=abi.LUT, lut=filmic_table(4096), sharpen=0.5)
     return Workload("c2_8k_raw12_bggr_whitepatch", width, height, abi.BGGR, abi.RAW12, 12, 256.0, p,
-                    abi.RGBA8, True, True)
+                    abi.RGBA8, True, True, fresh_frames=200)
 
 
-# ---- The same scene model on the GPU (torch), for large benchmark inputs ----
-
-def device_counts(width: int, height: int, pattern: int, black: float, bits: int, seed: int, device="cuda"):
-    """Raw counts [H, W] int32 on `device`: the scene model above evaluated with
-    torch (random choices from numpy's PCG64, noise from torch's generator)."""
-    import torch
-
-    rng = np.random.default_rng(np.random.PCG64(seed))
-    white = (1 << bits) - 1
-    ys = torch.arange(height, device=device, dtype=torch.float32)[:, None]
-    xs = torch.arange(width, device=device, dtype=torch.float32)[None, :]
-    base = rng.uniform(0.05, 0.35, 3)
-    gx = rng.uniform(-0.25, 0.25, 3) / max(width - 1, 1)
-    gy = rng.uniform(-0.25, 0.25, 3) / max(height - 1, 1)
-    img = torch.stack([base[c] + gx[c] * xs + gy[c] * ys for c in range(3)])  # [3, H, W]
-    for _ in range(8):
-        cx, cy = rng.uniform(0, width), rng.uniform(0, height)
-        sigma = rng.uniform(50.0, 300.0)
-        amp = torch.tensor(rng.uniform(0.05, 0.5, 3), device=device, dtype=torch.float32)
-        ex = torch.exp(-((xs - cx) ** 2) / (2 * sigma * sigma))
-        ey = torch.exp(-((ys - cy) ** 2) / (2 * sigma * sigma))
-        img += amp[:, None, None] * (ey * ex)[None]
-    for _ in range(64):
-        w = int(rng.uniform(0.02, 0.2) * width) + 1
-        h = int(rng.uniform(0.02, 0.2) * height) + 1
-        x0 = int(rng.uniform(0, max(width - w, 1)))
-        y0 = int(rng.uniform(0, max(height - h, 1)))
-        img[:, y0:y0 + h, x0:x0 + w] = torch.tensor(rng.uniform(0.0, 1.0, 3), device=device,
-                                                      dtype=torch.float32)[:, None, None]
-    img.clamp_(0.0, 1.0)
-    cxv, cyv = (width - 1) / 2.0, (height - 1) / 2.0
-    rc = math.hypot(cxv, cyv) or 1.0
-    r = torch.sqrt((xs - cxv) ** 2 + (ys - cyv) ** 2) / rc
-    vig = torch.cos(torch.atan(r * math.tan(_THETA_EDGE))) ** 4
-    colors = torch.tensor(_CFA_COLOR[pattern], device=device)
-    yi = torch.arange(height, device=device)[:, None]
-    xi = torch.arange(width, device=device)[None, :]
-    idx = colors[((yi & 1) << 1) | (xi & 1)]
-    sig = torch.gather(img, 0, idx[None])[0] * vig
-    gen = torch.Generator(device=device)
-    gen.manual_seed(seed)
-    dn = sig * (white - black)
-    electrons = torch.poisson(dn / 0.5, generator=gen)
-    dn = electrons * 0.5 + torch.randn(dn.shape, generator=gen, device=device) * 3.0
-    return torch.round(black + dn).clamp_(0, white).to(torch.int32)
-
-
-def device_pack(counts, fmt: int):
-    """Rows of `counts` (int32 [H, W] on the GPU) packed as `fmt`: uint8 [H * row] and the row bytes."""
-    import torch
-
-    h, w = counts.shape
-    if fmt == U8_FMT:
-        return counts.to(torch.uint8).reshape(-1), w
-    if fmt == U16_FMT:
-        return counts.to(torch.int16).view(torch.uint8).reshape(-1), 2 * w
-    if fmt == RAW10_FMT:
-        wp = (w + 3) // 4 * 4
-        c = torch.zeros((h, wp), dtype=torch.int32, device=counts.device)
-        c[:, :w] = counts
-        g = c.reshape(h, wp // 4, 4)
-        out = torch.empty((h, wp // 4, 5), dtype=torch.uint8, device=counts.device)
-        out[:, :, :4] = (g >> 2).to(torch.uint8)
-        out[:, :, 4] = ((g[:, :, 0] & 3) | ((g[:, :, 1] & 3) << 2) | ((g[:, :, 2] & 3) << 4) |
-                        ((g[:, :, 3] & 3) << 6)).to(torch.uint8)
-        return out.reshape(-1), 5 * (wp // 4)
-    wp = (w + 1) // 2 * 2
-    c = torch.zeros((h, wp), dtype=torch.int32, device=counts.device)
-    c[:, :w] = counts
-    g = c.reshape(h, wp // 2, 2)
-    out = torch.empty((h, wp // 2, 3), dtype=torch.uint8, device=counts.device)
-    out[:, :, :2] = (g >> 4).to(torch.uint8)
-    out[:, :, 2] = ((g[:, :, 0] & 15) | ((g[:, :, 1] & 15) << 4)).to(torch.uint8)
-    return out.reshape(-1), 3 * (wp // 2)
-
-
-U8_FMT, U16_FMT, RAW10_FMT, RAW12_FMT = abi.U8, abi.U16, abi.RAW10, abi.RAW12
 
 
 @dataclass

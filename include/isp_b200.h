@@ -347,6 +347,36 @@ ISP_B200_API int isp_b200_server_run_closed(isp_b200_server* server, double seco
 /* Finishes the frames in flight, then frees everything. */
 ISP_B200_API void isp_b200_server_destroy(isp_b200_server* server);
 
+/* ---- Synthetic frames ------------------------------------------------------
+ *
+ * Seeded raw frames rendered on the device, for throughput workloads that
+ * need fresh frames at rate; they play the part of the reference module's
+ * synthetic camera (modules/isp/src/synthetic_raw.cu, its render kernel),
+ * with the benchmark's scene instead of its test chart: a base level and
+ * gradient, 8 Gaussian blobs (sigma 50..300 px), 64 uniform rectangles, a
+ * cos^4 vignette (corner gain vignette_edge), mosaicked in `pattern`, scaled
+ * to [black, 2^bit_depth - 1], Poisson shot noise (gain counts per
+ * electron, 0: none) and Gaussian read noise (read_noise counts), rounded,
+ * clipped and packed in `format`. A frame is a pure function of its seed and
+ * settings. */
+typedef struct isp_synth_c {
+  int32_t width;
+  int32_t height;
+  int32_t format;
+  int32_t bit_depth;
+  int32_t pattern;
+  float black;
+  float gain;
+  float read_noise;
+  float vignette_edge;
+} isp_synth_c;
+
+ISP_B200_API void isp_b200_synth_default(isp_synth_c* config);
+/* Renders the frame of `seed` into `raw` (device memory, row stride `pitch`)
+ * on `stream`. ISP_EINVAL for settings that do not make a valid raw view. */
+ISP_B200_API int isp_b200_synthetic_raw(const isp_synth_c* config, uint64_t seed, void* raw, size_t pitch,
+                           void* stream);
+
 /* One frame without allocating memory. No reference counterpart: for callers
  * that cannot allocate device memory (cudaMalloc forbidden or unsafe where
  * they run, e.g. a host that owns every allocation or a real-time loop that
