@@ -102,3 +102,64 @@ def test_pipeline_frames_match_oracle(facade, tmp_path):
         assert part[:image_bytes] == exp.image.tobytes(), f"frame {f}: image"
         assert part[image_bytes:image_bytes + 4096] == exp.histogram.astype(np.uint32).tobytes(), f"frame {f}: histogram"
         assert part[image_bytes + 4096:] == exp.stats.astype(np.float32).tobytes(), f"frame {f}: statistics"
+
+
+# ---- The operator's work without the SDK (holoscan/isp/isp_op_core.hpp) -------
+
+@pytest.fixture(scope="module")
+def op_core(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("opcore") / "op_core_check")
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(PKG, "cpp", "include"),
+           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(CUDA, "include"),
+           os.path.join(ROOT, "tests", "cpp", "op_core_check.cpp"), "-L", PKG, "-lisp_b200",
+           "-L", os.path.join(CUDA, "lib64"), "-lcudart", f"-Wl,-rpath,{PKG}", f"-Wl,-rpath,{CUDA}/lib64", "-o", exe]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return exe
+
+
+def test_operator_configuration_checks(op_core):
+    c = _checks(op_core, "host")
+    assert c["config_ok"]["error"] == ""
+    assert c["config_max_size"]["error"] == "max_width and max_height must be 2..16384"
+    assert c["config_bit_depth"]["error"] == "bit_depth must be 0 (from the image) or 1..16"
+    assert c["config_packed_bits"]["error"] == "packed RAW10 and RAW12 samples have 10 and 12 bits"
+    assert c["config_params"]["error"] == "sharpen must be 0..4"
+
+
+def test_operator_describes_inputs_as_the_reference_does(op_core):
+    c = _checks(op_core, "host")
+    pad = c["u16_padded"]
+    assert (pad["error"], pad["width"], pad["height"], pad["pitch"], pad["format"], pad["bits"], pad["pattern"],
+            pad["span"], pad["contiguous"]) == ("", 64, 32, 160, abi.U16, 12, abi.GRBG, 160 * 31 + 128, 0)
+    assert c["u16_contiguous"]["contiguous"] == 1 and c["u16_contiguous"]["span"] == 64 * 32 * 2
+    assert c["mono_with_pattern"]["error"] == "" and c["mono_with_pattern"]["pattern"] == abi.BGGR
+    assert c["unknown_bits"]["bits"] == 16  # the container's bits when the image does not say
+    raw10 = c["raw10"]
+    assert (raw10["error"], raw10["width"], raw10["format"], raw10["bits"], raw10["span"]) == (
+        "", 80, abi.RAW10, 10, 112 * 31 + abi.raw_row_bytes(abi.RAW10, 80))
+    errors = {
+        "bad_encoding": "IspOp: unsupported raw encoding RGB8; use BAYER_RGGB, BAYER_BGGR, BAYER_GRBG, BAYER_GBRG, "
+                        "MONO8 or MONO16",
+        "mono_without_pattern": "IspOp: a MONO8 or MONO16 raw image needs the Bayer pattern in the configuration",
+        "pattern_disagrees": "IspOp: the image's pattern GRBG disagrees with the configured BGGR",
+        "element_vs_encoding": "IspOp: raw element type disagrees with its encoding",
+        "strided_row": "IspOp: raw samples within a row must be packed",
+        "overlap": "IspOp: raw rows overlap",
+        "too_large": "IspOp: raw image 4000x32 is outside 2x2 to the configured 3840x2160",
+        "misaligned": "IspOp: uint16 raw data must be aligned to 2 bytes",
+        "raw10_short_rows": "IspOp: packed rows of 100 bytes cannot hold 81 samples",
+        "elsewhere": "IspOp: raw images must be in host or CUDA memory",
+    }
+    for name, message in errors.items():
+        assert c[name]["error"] == message, name
+
+
+@pytest.mark.gpu
+def test_operator_stages_host_frames_and_counts_waits_and_copies(op_core):
+    g = _checks(op_core, "gpu")["gpu"]
+    assert g["error"] == "no error" and g["same"] == 1
+    # A pageable host frame: the producer's wait and the copy's wait, one copy;
+    # a pinned frame: one queued copy; a device frame: nothing.
+    assert (g["pageable_waits"], g["pageable_copies"]) == (2, 1)
+    assert (g["pinned_waits"], g["pinned_copies"]) == (0, 1)
+    assert (g["device_waits"], g["device_copies"]) == (0, 0)
