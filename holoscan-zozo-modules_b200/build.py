@@ -27,14 +27,26 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC
           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-DISP_B200_BUILD"]
 
 SOURCES = ["isp_batch.cu", "isp_batch_global_lut.cu", "isp_main_bilinear.cu", "isp_main_bilinear_sharpen.cu", "isp_main_malvar.cu", "isp_main_malvar_sharpen.cu",
-           "isp_awb.cu", "isp_kernels.cu", "isp_capi.cu", "isp_batch_host.cu", "isp_noalloc.cu", "isp_server.cu", "isp_synth.cu", "isp_params.cpp"]
+           "isp_awb.cu", "isp_kernels.cu", "isp_capi.cu", "isp_batch_host.cu", "isp_noalloc.cu", "isp_server.cu", "isp_synth.cu", "isp_params.cpp",
+           # the colour converter (the step after the ISP)
+           "cc/cc_direct_yuv.cu", "cc/cc_direct_rgb.cu", "cc/cc_direct_gray.cu", "cc/cc_resample.cu", "cc/cc_capi.cu",
+           "cc/cc_plan.cpp"]
+
+
+def _headers(folder: str) -> list:
+    return [os.path.join(folder, f) for f in os.listdir(folder) if f.endswith((".cuh", ".hpp"))]
 
 
 def _compile(src: str, verbose: bool) -> str:
-    out = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
+    out = os.path.join(OBJ, os.path.splitext(src)[0].replace("/", "_") + ".o")
     path = os.path.join(CSRC, src)
-    deps = [path] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp"))]
+    # A source depends on the headers of its own folder and of csrc/ (the
+    # converter's folder includes the ISP's host helpers, not the reverse).
+    folder = os.path.dirname(path)
+    deps = [path] + _headers(CSRC) + (_headers(folder) if folder != CSRC else [])
     deps.append(os.path.join(ROOT, "include", "isp_b200.h"))
+    if folder != CSRC:
+        deps.append(os.path.join(ROOT, "include", "cc_b200.h"))
     if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
         return out
     cmd = [NVCC, *ARCH, *COMMON, "-c", path, "-o", out]

@@ -1,0 +1,322 @@
+// cc_common.cuh - the B200 colour converter's plan and per-pixel arithmetic.
+//
+// One conversion is defined as in holoscan::color_convert
+// (modules/color-convert/include/holoscan/color_convert/conversion.hpp:9-27,
+// arithmetic in src/kernel_math.hpp:70-370):
+//   1. a source pixel decodes to its format's samples (Y Cb Cr, R G B or
+//      luma; chroma from the chroma sample covering the pixel; 16-bit
+//      samples divided by 257; alpha 255 unless stored);
+//   2. a destination pixel inside the content rectangle samples the source
+//      rectangle (nearest, bilinear or area); outside it takes the fill;
+//   3. the samples go through one 3x4 affine map to the destination's
+//      model (none between equal models), are rounded half up and clamped;
+//      a subsampled destination stores the mean chroma of its block.
+// Every sum and product below is a separate IEEE single operation, in the
+// reference's order (the library is compiled with --fmad=false), so the
+// kernels give the reference's bytes.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "cc_b200.h"
+
+#if defined(__CUDACC__)
+#define CC_HD __host__ __device__ __forceinline__
+#else
+#define CC_HD inline
+#endif
+
+namespace cc_b200 {
+
+enum Model : int { kYuv = 0, kRgb = 1, kGray = 2 };
+
+struct FormatInfo {
+  int model, planes, shift_x, shift_y, bytes, channels;
+};
+
+// pixel_format.hpp:58-84.
+CC_HD constexpr FormatInfo info_of(int f) {
+  return f == CC_NV12    ? FormatInfo{kYuv, 2, 1, 1, 1, 1}
+         : f == CC_NV16  ? FormatInfo{kYuv, 2, 1, 0, 1, 1}
+         : f == CC_I420  ? FormatInfo{kYuv, 3, 1, 1, 1, 1}
+         : f == CC_YUYV  ? FormatInfo{kYuv, 1, 1, 0, 1, 2}
+         : f == CC_UYVY  ? FormatInfo{kYuv, 1, 1, 0, 1, 2}
+         : f == CC_RGB8  ? FormatInfo{kRgb, 1, 0, 0, 1, 3}
+         : f == CC_BGR8  ? FormatInfo{kRgb, 1, 0, 0, 1, 3}
+         : f == CC_RGBA8 ? FormatInfo{kRgb, 1, 0, 0, 1, 4}
+         : f == CC_BGRA8 ? FormatInfo{kRgb, 1, 0, 0, 1, 4}
+         : f == CC_MONO8 ? FormatInfo{kGray, 1, 0, 0, 1, 1}
+         : f == CC_MONO16 ? FormatInfo{kGray, 1, 0, 0, 2, 1}
+                          : FormatInfo{kRgb, 1, 0, 0, 2, 3};
+}
+
+struct Image {
+  int format, width, height;
+  uint8_t* data[3];
+  size_t pitch[3];
+};
+
+// Everything one conversion needs, by value in the kernel's parameters.
+struct Plan {
+  Image src, dst;
+  int mode;
+  int sx0, sy0, sx1, sy1;  // source rectangle, inclusive bounds
+  float scale_x, scale_y;  // source pixels per content pixel
+  int cx0, cy0, cx1, cy1;  // content rectangle [cx0, cx1) x [cy0, cy1)
+  float m[9], o[3];
+  int identity;
+  float fill[4];  // in the destination's model
+  int bsx, bsy;   // log2 of the pixels one destination chroma sample covers
+};
+
+struct Px {
+  float c0, c1, c2, a;
+};
+
+#if defined(__CUDACC__)
+
+__device__ __forceinline__ float byte_f(uint32_t b) { return static_cast<float>(b); }
+
+// Rounded half up and clamped to 0..255 (kernel_math.hpp:89-92): the floor of
+// v + 0.5 saturated by the conversion to unsigned, then capped.
+__device__ __forceinline__ uint32_t code8(float v) {
+  const uint32_t r = __float2uint_rd(v + 0.5F);
+  return r < 255U ? r : 255U;
+}
+
+// 16-bit codes: the floor of v * 257 + 0.5, clamped to 0..65535 (:94-97).
+__device__ __forceinline__ uint32_t code16(float v) {
+  const float p = v * 257.0F;
+  const uint32_t r = __float2uint_rd(p + 0.5F);
+  return r < 65535U ? r : 65535U;
+}
+
+// A 16-bit little-endian sample on the 8-bit scale (:99-104), read byte-wise
+// since a pitched row of 16-bit samples need not be 2-byte aligned.
+__device__ __forceinline__ float word_sample(const uint8_t* p) {
+  const uint32_t v = static_cast<uint32_t>(__ldg(p)) | (static_cast<uint32_t>(__ldg(p + 1)) << 8);
+  return __fdiv_rn(static_cast<float>(v), 257.0F);
+}
+
+__device__ __forceinline__ const uint8_t* row_of(const Image& img, int plane, int y) {
+  return img.data[plane] + static_cast<size_t>(y) * img.pitch[plane];
+}
+
+// Pixel (x, y) of a source image of format kF, in its own samples (:112-161).
+template <int kF>
+__device__ __forceinline__ Px load_px(const Image& img, int x, int y) {
+  const uint8_t* row = row_of(img, 0, y);
+  if constexpr (kF == CC_NV12 || kF == CC_NV16) {
+    const uint8_t* uv = row_of(img, 1, kF == CC_NV12 ? (y >> 1) : y) + 2 * (x >> 1);
+    return {byte_f(__ldg(row + x)), byte_f(__ldg(uv)), byte_f(__ldg(uv + 1)), 255.0F};
+  } else if constexpr (kF == CC_I420) {
+    const int cx = x >> 1, cy = y >> 1;
+    return {byte_f(__ldg(row + x)), byte_f(__ldg(row_of(img, 1, cy) + cx)), byte_f(__ldg(row_of(img, 2, cy) + cx)),
+            255.0F};
+  } else if constexpr (kF == CC_YUYV) {
+    const uint8_t* pair = row + 4 * (x >> 1);
+    return {byte_f(__ldg(pair + 2 * (x & 1))), byte_f(__ldg(pair + 1)), byte_f(__ldg(pair + 3)), 255.0F};
+  } else if constexpr (kF == CC_UYVY) {
+    const uint8_t* pair = row + 4 * (x >> 1);
+    return {byte_f(__ldg(pair + 1 + 2 * (x & 1))), byte_f(__ldg(pair)), byte_f(__ldg(pair + 2)), 255.0F};
+  } else if constexpr (kF == CC_RGB8 || kF == CC_BGR8) {
+    const uint8_t* p = row + 3 * x;
+    const float a = byte_f(__ldg(p)), b = byte_f(__ldg(p + 1)), c = byte_f(__ldg(p + 2));
+    return kF == CC_RGB8 ? Px{a, b, c, 255.0F} : Px{c, b, a, 255.0F};
+  } else if constexpr (kF == CC_RGBA8 || kF == CC_BGRA8) {
+    const uint8_t* p = row + 4 * x;
+    const float a = byte_f(__ldg(p)), b = byte_f(__ldg(p + 1)), c = byte_f(__ldg(p + 2));
+    const float al = byte_f(__ldg(p + 3));
+    return kF == CC_RGBA8 ? Px{a, b, c, al} : Px{c, b, a, al};
+  } else if constexpr (kF == CC_MONO8) {
+    return {byte_f(__ldg(row + x)), 0.0F, 0.0F, 255.0F};
+  } else if constexpr (kF == CC_MONO16) {
+    return {word_sample(row + 2 * x), 0.0F, 0.0F, 255.0F};
+  } else {
+    const uint8_t* p = row + 6 * x;
+    return {word_sample(p), word_sample(p + 2), word_sample(p + 4), 255.0F};
+  }
+}
+
+// c = m s + o on the colour samples, each row summed left to right; alpha
+// passes through (:236-244).
+__device__ __forceinline__ Px apply_affine(const Plan& p, Px s) {
+  if (p.identity) return s;
+  Px r;
+  r.c0 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p.m[0], s.c0), __fmul_rn(p.m[1], s.c1)), __fmul_rn(p.m[2], s.c2)),
+                   p.o[0]);
+  r.c1 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p.m[3], s.c0), __fmul_rn(p.m[4], s.c1)), __fmul_rn(p.m[5], s.c2)),
+                   p.o[1]);
+  r.c2 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p.m[6], s.c0), __fmul_rn(p.m[7], s.c1)), __fmul_rn(p.m[8], s.c2)),
+                   p.o[2]);
+  r.a = s.a;
+  return r;
+}
+
+__device__ __forceinline__ void put_word(uint8_t* q, uint32_t w) {
+  q[0] = static_cast<uint8_t>(w & 0xFFU);
+  q[1] = static_cast<uint8_t>(w >> 8);
+}
+
+// Everything but chroma of pixel (x, y) of a destination of format kF (the
+// luma of a YCbCr one), :256-307.
+template <int kF>
+__device__ __forceinline__ void store_px(const Image& img, int x, int y, const Px& v) {
+  uint8_t* row = img.data[0] + static_cast<size_t>(y) * img.pitch[0];
+  if constexpr (kF == CC_NV12 || kF == CC_NV16 || kF == CC_I420 || kF == CC_MONO8) {
+    row[x] = static_cast<uint8_t>(code8(v.c0));
+  } else if constexpr (kF == CC_YUYV) {
+    row[4 * (x >> 1) + 2 * (x & 1)] = static_cast<uint8_t>(code8(v.c0));
+  } else if constexpr (kF == CC_UYVY) {
+    row[4 * (x >> 1) + 1 + 2 * (x & 1)] = static_cast<uint8_t>(code8(v.c0));
+  } else if constexpr (kF == CC_RGB8 || kF == CC_BGR8) {
+    uint8_t* q = row + 3 * x;
+    const bool bgr = kF == CC_BGR8;
+    q[0] = static_cast<uint8_t>(code8(bgr ? v.c2 : v.c0));
+    q[1] = static_cast<uint8_t>(code8(v.c1));
+    q[2] = static_cast<uint8_t>(code8(bgr ? v.c0 : v.c2));
+  } else if constexpr (kF == CC_RGBA8 || kF == CC_BGRA8) {
+    const bool bgr = kF == CC_BGRA8;
+    const uint32_t w = code8(bgr ? v.c2 : v.c0) | (code8(v.c1) << 8) | (code8(bgr ? v.c0 : v.c2) << 16) |
+                       (code8(v.a) << 24);
+    uint8_t* q = row + 4 * x;
+    if ((reinterpret_cast<uintptr_t>(q) & 3U) == 0U) {
+      *reinterpret_cast<uint32_t*>(q) = w;
+    } else {
+      q[0] = static_cast<uint8_t>(w);
+      q[1] = static_cast<uint8_t>(w >> 8);
+      q[2] = static_cast<uint8_t>(w >> 16);
+      q[3] = static_cast<uint8_t>(w >> 24);
+    }
+  } else if constexpr (kF == CC_MONO16) {
+    put_word(row + 2 * x, code16(v.c0));
+  } else {
+    uint8_t* q = row + 6 * x;
+    put_word(q, code16(v.c0));
+    put_word(q + 2, code16(v.c1));
+    put_word(q + 4, code16(v.c2));
+  }
+}
+
+// Chroma sample (cx, cy) of a YCbCr destination (:311-341).
+template <int kF>
+__device__ __forceinline__ void store_chroma(const Image& img, int cx, int cy, float cb, float cr) {
+  if constexpr (kF == CC_NV12 || kF == CC_NV16) {
+    uint8_t* q = img.data[1] + static_cast<size_t>(cy) * img.pitch[1] + 2 * cx;
+    q[0] = static_cast<uint8_t>(code8(cb));
+    q[1] = static_cast<uint8_t>(code8(cr));
+  } else if constexpr (kF == CC_I420) {
+    img.data[1][static_cast<size_t>(cy) * img.pitch[1] + cx] = static_cast<uint8_t>(code8(cb));
+    img.data[2][static_cast<size_t>(cy) * img.pitch[2] + cx] = static_cast<uint8_t>(code8(cr));
+  } else if constexpr (kF == CC_YUYV) {
+    uint8_t* q = img.data[0] + static_cast<size_t>(cy) * img.pitch[0] + 4 * cx;
+    q[1] = static_cast<uint8_t>(code8(cb));
+    q[3] = static_cast<uint8_t>(code8(cr));
+  } else if constexpr (kF == CC_UYVY) {
+    uint8_t* q = img.data[0] + static_cast<size_t>(cy) * img.pitch[0] + 4 * cx;
+    q[0] = static_cast<uint8_t>(code8(cb));
+    q[2] = static_cast<uint8_t>(code8(cr));
+  }
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// sum + s w per sample, product then sum, each rounded (:163-165).
+__device__ __forceinline__ Px accumulate(Px sum, const Px& s, float w) {
+  return {__fadd_rn(sum.c0, __fmul_rn(s.c0, w)), __fadd_rn(sum.c1, __fmul_rn(s.c1, w)),
+          __fadd_rn(sum.c2, __fmul_rn(s.c2, w)), __fadd_rn(sum.a, __fmul_rn(s.a, w))};
+}
+
+// Weight of source pixel [i, i + 1) in the footprint [lo, hi) (:168-172).
+__device__ __forceinline__ float covered(int i, float lo, float hi) {
+  const float fi = static_cast<float>(i);
+  const float fj = static_cast<float>(i + 1);
+  const float a = fi > lo ? fi : lo;
+  const float b = fj < hi ? fj : hi;
+  return b > a ? __fsub_rn(b, a) : 0.0F;
+}
+
+// The source sampled for content pixel (dx, dy) (:175-233), resize mode kMode.
+template <int kSrc, int kMode>
+__device__ __forceinline__ Px sample_px(const Plan& p, int dx, int dy) {
+  const float rx = static_cast<float>(dx - p.cx0);
+  const float ry = static_cast<float>(dy - p.cy0);
+  const float x0 = static_cast<float>(p.sx0);
+  const float y0 = static_cast<float>(p.sy0);
+  if constexpr (kMode == CC_NEAREST) {
+    const int sx = clampi(static_cast<int>(floorf(__fadd_rn(x0, __fmul_rn(__fadd_rn(rx, 0.5F), p.scale_x)))), p.sx0, p.sx1);
+    const int sy = clampi(static_cast<int>(floorf(__fadd_rn(y0, __fmul_rn(__fadd_rn(ry, 0.5F), p.scale_y)))), p.sy0, p.sy1);
+    return load_px<kSrc>(p.src, sx, sy);
+  } else if constexpr (kMode == CC_BILINEAR) {
+    const float fx = __fsub_rn(__fadd_rn(x0, __fmul_rn(__fadd_rn(rx, 0.5F), p.scale_x)), 0.5F);
+    const float fy = __fsub_rn(__fadd_rn(y0, __fmul_rn(__fadd_rn(ry, 0.5F), p.scale_y)), 0.5F);
+    const float bx = floorf(fx);
+    const float by = floorf(fy);
+    const float ax = __fsub_rn(fx, bx);
+    const float ay = __fsub_rn(fy, by);
+    const int ix = static_cast<int>(bx);
+    const int iy = static_cast<int>(by);
+    const int xa = clampi(ix, p.sx0, p.sx1);
+    const int xb = clampi(ix + 1, p.sx0, p.sx1);
+    const int ya = clampi(iy, p.sy0, p.sy1);
+    const int yb = clampi(iy + 1, p.sy0, p.sy1);
+    const float bx1 = __fsub_rn(1.0F, ax);
+    const float by1 = __fsub_rn(1.0F, ay);
+    const float w00 = __fmul_rn(bx1, by1);
+    const float w10 = __fmul_rn(ax, by1);
+    const float w01 = __fmul_rn(bx1, ay);
+    const float w11 = __fmul_rn(ax, ay);
+    // Taps of zero weight are skipped, as the definition does.
+    Px s{0.0F, 0.0F, 0.0F, 0.0F};
+    if (w00 != 0.0F) s = accumulate(s, load_px<kSrc>(p.src, xa, ya), w00);
+    if (w10 != 0.0F) s = accumulate(s, load_px<kSrc>(p.src, xb, ya), w10);
+    if (w01 != 0.0F) s = accumulate(s, load_px<kSrc>(p.src, xa, yb), w01);
+    if (w11 != 0.0F) s = accumulate(s, load_px<kSrc>(p.src, xb, yb), w11);
+    return s;
+  } else {
+    // Area: the footprint [lo, hi) on each axis, inside the source rectangle.
+    const float lx = __fadd_rn(x0, __fmul_rn(rx, p.scale_x));
+    const float ly = __fadd_rn(y0, __fmul_rn(ry, p.scale_y));
+    const float right = static_cast<float>(p.sx1 + 1);
+    const float bottom = static_cast<float>(p.sy1 + 1);
+    const float lxs = __fadd_rn(lx, p.scale_x);
+    const float lys = __fadd_rn(ly, p.scale_y);
+    const float hx = lxs < right ? lxs : right;
+    const float hy = lys < bottom ? lys : bottom;
+    const int ix0 = clampi(static_cast<int>(floorf(lx)), p.sx0, p.sx1);
+    const int iy0 = clampi(static_cast<int>(floorf(ly)), p.sy0, p.sy1);
+    Px s{0.0F, 0.0F, 0.0F, 0.0F};
+    float total = 0.0F;
+    for (int y = iy0; y <= p.sy1 && static_cast<float>(y) < hy; ++y) {
+      const float wy = covered(y, ly, hy);
+      for (int x = ix0; x <= p.sx1 && static_cast<float>(x) < hx; ++x) {
+        const float w = __fmul_rn(covered(x, lx, hx), wy);
+        if (w != 0.0F) {
+          s = accumulate(s, load_px<kSrc>(p.src, x, y), w);
+          total = __fadd_rn(total, w);
+        }
+      }
+    }
+    if (total <= 0.0F) return load_px<kSrc>(p.src, ix0, iy0);
+    return {__fdiv_rn(s.c0, total), __fdiv_rn(s.c1, total), __fdiv_rn(s.c2, total), __fdiv_rn(s.a, total)};
+  }
+}
+
+__device__ __forceinline__ bool in_content(const Plan& p, int x, int y) {
+  return x >= p.cx0 && x < p.cx1 && y >= p.cy0 && y < p.cy1;
+}
+
+#endif  // __CUDACC__
+
+// Host side (cc_plan.cpp): names, geometry, checks and the plan.
+int make_plan(const cc_image_c* src, const cc_image_c* dst, const cc_params_c* params, Plan* plan);
+int compute_mapping(int sw, int sh, int w, int h, int dst_format, const cc_params_c* params, cc_mapping_c* out);
+int validate(const cc_image_c* src, const cc_image_c* dst, const cc_params_c* params);
+bool known_format(int f);
+
+// Kernel launchers (cc_kernels*.cu).
+int launch_convert(const Plan& plan, void* stream);
+int launch_pattern(uint8_t* data, size_t pitch, int width, int height, uint32_t frame, void* stream);
+
+}  // namespace cc_b200

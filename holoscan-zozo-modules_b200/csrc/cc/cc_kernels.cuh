@@ -1,0 +1,255 @@
+// cc_kernels.cuh - the colour converter's kernels.
+//
+// Direct path (source and content the same size on both axes, which is every
+// plain format conversion): whatever the resize mode, each destination pixel
+// then reads exactly the one source pixel under it (bilinear and area
+// weights are exactly 1 and 0 there), so a thread converts a group of four
+// pixels across (two rows of them for a 4:2:0 destination: two whole chroma
+// blocks) with both formats known at compile time, and writes each row's
+// segment with 32-bit stores where it is aligned.
+//
+// Resample path: one thread per destination block (a pixel, or the pixels
+// sharing a chroma sample), the source format and resize mode known at
+// compile time, the destination's stores chosen at run time.
+#pragma once
+
+#include "cc_common.cuh"
+
+namespace cc_b200 {
+
+constexpr int kGroupX = 4;     // pixels across per direct-path thread
+constexpr int kThreadsX = 32;  // CTA shape for both paths
+constexpr int kThreadsY = 8;
+
+__device__ __forceinline__ bool yuv_dst(int f) { return f <= CC_UYVY; }
+
+// Writes n bytes held little-endian in w to q: whole words where q is
+// 4-byte aligned, bytes otherwise.
+template <int kWords>
+__device__ __forceinline__ void put_segment(uint8_t* q, const uint32_t (&w)[kWords], int n) {
+  if ((reinterpret_cast<uintptr_t>(q) & 3U) == 0U && n == 4 * kWords) {
+#pragma unroll
+    for (int i = 0; i < kWords; ++i) reinterpret_cast<uint32_t*>(q)[i] = w[i];
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4 * kWords; ++i) {
+      if (i < n) q[i] = static_cast<uint8_t>(w[i >> 2] >> (8 * (i & 3)));
+    }
+  }
+}
+
+__device__ __forceinline__ void set_byte(uint32_t* w, int i, uint32_t b) { w[i >> 2] |= b << (8 * (i & 3)); }
+
+// One row segment of up to four destination pixels (v[0..n)) of format kDst
+// at (x, y); chroma of YCbCr formats is written separately, except for the
+// packed 4:2:2 ones, whose row words interleave it (cb/cr per pixel pair).
+template <int kDst>
+__device__ __forceinline__ void store_row4(const Image& img, int x, int y, const Px (&v)[kGroupX], int n,
+                                           const uint32_t (&cb)[2], const uint32_t (&cr)[2]) {
+  uint8_t* row = img.data[0] + static_cast<size_t>(y) * img.pitch[0];
+  constexpr FormatInfo fi = info_of(kDst);
+  constexpr int kBpp = fi.model == kYuv && fi.channels == 2 ? 2 : fi.channels * fi.bytes;
+  constexpr int kWords = kBpp;  // 4 pixels x kBpp bytes = kBpp words
+  uint32_t w[kWords];
+#pragma unroll
+  for (int i = 0; i < kWords; ++i) w[i] = 0U;
+#pragma unroll
+  for (int i = 0; i < kGroupX; ++i) {
+    if constexpr (kDst == CC_NV12 || kDst == CC_NV16 || kDst == CC_I420 || kDst == CC_MONO8) {
+      set_byte(w, i, code8(v[i].c0));
+    } else if constexpr (kDst == CC_YUYV) {
+      set_byte(w, 2 * i, code8(v[i].c0));
+      set_byte(w, 2 * i + 1, (i & 1) ? cr[i >> 1] : cb[i >> 1]);
+    } else if constexpr (kDst == CC_UYVY) {
+      set_byte(w, 2 * i + 1, code8(v[i].c0));
+      set_byte(w, 2 * i, (i & 1) ? cr[i >> 1] : cb[i >> 1]);
+    } else if constexpr (kDst == CC_RGB8 || kDst == CC_BGR8) {
+      const bool bgr = kDst == CC_BGR8;
+      set_byte(w, 3 * i, code8(bgr ? v[i].c2 : v[i].c0));
+      set_byte(w, 3 * i + 1, code8(v[i].c1));
+      set_byte(w, 3 * i + 2, code8(bgr ? v[i].c0 : v[i].c2));
+    } else if constexpr (kDst == CC_RGBA8 || kDst == CC_BGRA8) {
+      const bool bgr = kDst == CC_BGRA8;
+      w[i] = code8(bgr ? v[i].c2 : v[i].c0) | (code8(v[i].c1) << 8) | (code8(bgr ? v[i].c0 : v[i].c2) << 16) |
+             (code8(v[i].a) << 24);
+    } else if constexpr (kDst == CC_MONO16) {
+      const uint32_t c = code16(v[i].c0);
+      set_byte(w, 2 * i, c & 0xFFU);
+      set_byte(w, 2 * i + 1, c >> 8);
+    } else {
+      const uint32_t r = code16(v[i].c0), g = code16(v[i].c1), b = code16(v[i].c2);
+      set_byte(w, 6 * i, r & 0xFFU);
+      set_byte(w, 6 * i + 1, r >> 8);
+      set_byte(w, 6 * i + 2, g & 0xFFU);
+      set_byte(w, 6 * i + 3, g >> 8);
+      set_byte(w, 6 * i + 4, b & 0xFFU);
+      set_byte(w, 6 * i + 5, b >> 8);
+    }
+  }
+  put_segment<kWords>(row + static_cast<size_t>(x) * kBpp, w, n * kBpp);
+}
+
+// Direct path: thread (gx, gy) converts pixels [4 gx, 4 gx + 4) of rows
+// [gy << bsy, (gy + 1) << bsy).
+template <int kSrc, int kDst>
+__global__ void __launch_bounds__(kThreadsX* kThreadsY) cc_direct_kernel(const __grid_constant__ Plan p, int groups_x,
+                                                                         int groups_y) {
+  const int gx = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+  const int gy = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
+  if (gx >= groups_x || gy >= groups_y) return;
+  constexpr FormatInfo fi = info_of(kDst);
+  constexpr bool kYuvDst = fi.model == kYuv;
+  constexpr int kRows = kYuvDst ? (1 << fi.shift_y) : 1;
+  const int x0 = gx * kGroupX;
+  const int y0 = gy * kRows;
+  const int n = p.dst.width - x0 < kGroupX ? p.dst.width - x0 : kGroupX;
+  // Source offset of destination pixel (x, y) inside the content.
+  const int ox = p.sx0 - p.cx0;
+  const int oy = p.sy0 - p.cy0;
+  float cbs[2] = {0.0F, 0.0F}, crs[2] = {0.0F, 0.0F};
+  int rows = 0;
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    const int y = y0 + r;
+    if (r > 0 && y >= p.dst.height) break;
+    ++rows;
+    Px v[kGroupX];
+    const bool row_in = y >= p.cy0 && y < p.cy1;
+#pragma unroll
+    for (int i = 0; i < kGroupX; ++i) {
+      const int x = x0 + i;
+      if (i < n && row_in && x >= p.cx0 && x < p.cx1) {
+        v[i] = apply_affine(p, load_px<kSrc>(p.src, x + ox, y + oy));
+      } else {
+        v[i] = Px{p.fill[0], p.fill[1], p.fill[2], p.fill[3]};
+      }
+      if constexpr (kYuvDst) {
+        if (i < n) {
+          cbs[i >> 1] = __fadd_rn(cbs[i >> 1], v[i].c1);
+          crs[i >> 1] = __fadd_rn(crs[i >> 1], v[i].c2);
+        }
+      }
+    }
+    if constexpr (kDst == CC_YUYV || kDst == CC_UYVY) {
+      // One row per block: the chroma of each pixel pair is known now.
+      uint32_t cb[2], cr[2];
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const float cnt = n - 2 * b >= 2 ? 2.0F : 1.0F;
+        cb[b] = code8(__fdiv_rn(cbs[b], cnt));
+        cr[b] = code8(__fdiv_rn(crs[b], cnt));
+      }
+      store_row4<kDst>(p.dst, x0, y, v, n, cb, cr);
+    } else {
+      const uint32_t none[2] = {0U, 0U};
+      store_row4<kDst>(p.dst, x0, y, v, n, none, none);
+    }
+  }
+  if constexpr (kDst == CC_NV12 || kDst == CC_NV16 || kDst == CC_I420) {
+    const int cx = x0 >> 1;
+    const int cy = y0 >> fi.shift_y;
+    const int nb = (n + 1) >> 1;  // chroma samples in this group: 1 or 2
+    uint32_t code[2][2];
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int cols = n - 2 * b >= 2 ? 2 : 1;
+      const float cnt = static_cast<float>(cols * rows);
+      code[b][0] = code8(__fdiv_rn(cbs[b], cnt));
+      code[b][1] = code8(__fdiv_rn(crs[b], cnt));
+    }
+    if constexpr (kDst == CC_I420) {
+      uint8_t* u = p.dst.data[1] + static_cast<size_t>(cy) * p.dst.pitch[1] + cx;
+      uint8_t* vv = p.dst.data[2] + static_cast<size_t>(cy) * p.dst.pitch[2] + cx;
+      const uint32_t uw[1] = {code[0][0] | (code[1][0] << 8)};
+      const uint32_t vw[1] = {code[0][1] | (code[1][1] << 8)};
+      if (nb == 2 && (reinterpret_cast<uintptr_t>(u) & 1U) == 0U && (reinterpret_cast<uintptr_t>(vv) & 1U) == 0U) {
+        *reinterpret_cast<uint16_t*>(u) = static_cast<uint16_t>(uw[0]);
+        *reinterpret_cast<uint16_t*>(vv) = static_cast<uint16_t>(vw[0]);
+      } else {
+        for (int b = 0; b < nb; ++b) {
+          u[b] = static_cast<uint8_t>(code[b][0]);
+          vv[b] = static_cast<uint8_t>(code[b][1]);
+        }
+      }
+    } else {
+      uint8_t* q = p.dst.data[1] + static_cast<size_t>(cy) * p.dst.pitch[1] + 2 * cx;
+      const uint32_t w[1] = {code[0][0] | (code[0][1] << 8) | (code[1][0] << 16) | (code[1][1] << 24)};
+      put_segment<1>(q, w, 2 * nb);
+    }
+  }
+}
+
+// Resample path helpers: the destination's stores chosen at run time.
+__device__ __forceinline__ void store_any(const Image& img, int x, int y, const Px& v) {
+  switch (img.format) {
+    case CC_NV12: store_px<CC_NV12>(img, x, y, v); break;
+    case CC_NV16: store_px<CC_NV16>(img, x, y, v); break;
+    case CC_I420: store_px<CC_I420>(img, x, y, v); break;
+    case CC_YUYV: store_px<CC_YUYV>(img, x, y, v); break;
+    case CC_UYVY: store_px<CC_UYVY>(img, x, y, v); break;
+    case CC_RGB8: store_px<CC_RGB8>(img, x, y, v); break;
+    case CC_BGR8: store_px<CC_BGR8>(img, x, y, v); break;
+    case CC_RGBA8: store_px<CC_RGBA8>(img, x, y, v); break;
+    case CC_BGRA8: store_px<CC_BGRA8>(img, x, y, v); break;
+    case CC_MONO8: store_px<CC_MONO8>(img, x, y, v); break;
+    case CC_MONO16: store_px<CC_MONO16>(img, x, y, v); break;
+    default: store_px<CC_RGB16>(img, x, y, v); break;
+  }
+}
+
+__device__ __forceinline__ void store_chroma_any(const Image& img, int cx, int cy, float cb, float cr) {
+  switch (img.format) {
+    case CC_NV12: store_chroma<CC_NV12>(img, cx, cy, cb, cr); break;
+    case CC_NV16: store_chroma<CC_NV16>(img, cx, cy, cb, cr); break;
+    case CC_I420: store_chroma<CC_I420>(img, cx, cy, cb, cr); break;
+    case CC_YUYV: store_chroma<CC_YUYV>(img, cx, cy, cb, cr); break;
+    default: store_chroma<CC_UYVY>(img, cx, cy, cb, cr); break;
+  }
+}
+
+template <int kSrc, int kMode>
+__device__ __forceinline__ Px pixel_at(const Plan& p, int x, int y) {
+  if (!in_content(p, x, y)) return Px{p.fill[0], p.fill[1], p.fill[2], p.fill[3]};
+  return apply_affine(p, sample_px<kSrc, kMode>(p, x, y));
+}
+
+// Resample path: thread (bx, by) converts destination block (bx, by)
+// (kernel_math.hpp:345-370).
+template <int kSrc, int kMode>
+__global__ void __launch_bounds__(kThreadsX* kThreadsY) cc_resample_kernel(const __grid_constant__ Plan p, int across,
+                                                                           int down) {
+  const int bx = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+  const int by = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
+  if (bx >= across || by >= down) return;
+  if (!yuv_dst(p.dst.format)) {
+    store_any(p.dst, bx, by, pixel_at<kSrc, kMode>(p, bx, by));
+    return;
+  }
+  const int x0 = bx << p.bsx;
+  const int y0 = by << p.bsy;
+  const int x1 = min(x0 + (1 << p.bsx), p.dst.width);
+  const int y1 = min(y0 + (1 << p.bsy), p.dst.height);
+  float cb = 0.0F, cr = 0.0F;
+  int n = 0;
+  for (int y = y0; y < y1; ++y) {
+    for (int x = x0; x < x1; ++x) {
+      const Px v = pixel_at<kSrc, kMode>(p, x, y);
+      store_any(p.dst, x, y, v);
+      cb = __fadd_rn(cb, v.c1);
+      cr = __fadd_rn(cr, v.c2);
+      ++n;
+    }
+  }
+  const float cnt = static_cast<float>(n);
+  store_chroma_any(p.dst, bx, by, __fdiv_rn(cb, cnt), __fdiv_rn(cr, cnt));
+}
+
+// Launchers of each source format's direct kernels (cc_direct_*.cu) and of
+// the resample kernels (cc_resample.cu): a kernel pointer or null.
+const void* direct_kernel(int src, int dst);
+const void* direct_kernel_yuv(int src, int dst);
+const void* direct_kernel_rgb(int src, int dst);
+const void* direct_kernel_gray(int src, int dst);
+const void* resample_kernel(int src, int mode);
+
+}  // namespace cc_b200

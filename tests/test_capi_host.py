@@ -1,5 +1,5 @@
 """The C-ABI library without a GPU: it loads, exports every entry point that
-include/isp_b200.h declares, and its host-side settings logic (defaults,
+include/isp_b200.h and include/cc_b200.h declare, and its host-side settings logic (defaults,
 validation and messages, row sizes, tone tables) is the reference's
 (modules/isp/src/isp_params.cpp:85-237), checked against the oracle and, where
 it is built, the reference itself."""
@@ -19,18 +19,19 @@ from isp_b200 import abi
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_functions():
-    text = open(os.path.join(ROOT, "include", "isp_b200.h")).read()
+def declared_functions(header="isp_b200.h", prefix="isp_b200_"):
+    text = open(os.path.join(ROOT, "include", header)).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(isp_b200_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(" + prefix + r"\w+)\s*\(", text)))
 
 
-def test_library_exports_every_declared_symbol():
+@pytest.mark.parametrize("header,prefix,least", [("isp_b200.h", "isp_b200_", 12), ("cc_b200.h", "cc_b200_", 17)])
+def test_library_exports_every_declared_symbol(header, prefix, least):
     lib = isp_b200.lib()
-    names = declared_functions()
-    assert len(names) >= 12
+    names = declared_functions(header, prefix)
+    assert len(names) >= least
     for name in names:
-        assert hasattr(lib, name), f"{name} is declared in include/isp_b200.h but not exported"
+        assert hasattr(lib, name), f"{name} is declared in include/{header} but not exported"
     assert lib.isp_b200_abi_version() == abi.ABI_VERSION
 
 
