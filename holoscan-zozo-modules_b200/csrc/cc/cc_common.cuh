@@ -76,27 +76,67 @@ struct Px {
 
 #if defined(__CUDACC__)
 
-__device__ __forceinline__ float byte_f(uint32_t b) { return static_cast<float>(b); }
+// Integers to floats and back without the conversion unit (a quarter of the
+// FP32 rate): 2^23 + k has k in its low mantissa bits for 0 <= k < 2^23, so
+// a byte b becomes the float b exactly as (2^23 + b) - 2^23, and a float c in
+// [0, 2^23) becomes floor(c) as the mantissa of c + 2^23 rounded down.
+constexpr uint32_t kTwo23Bits = 0x4B000000U;
+constexpr float kTwo23 = 8388608.0F;
 
-// Rounded half up and clamped to 0..255 (kernel_math.hpp:89-92): the floor of
-// v + 0.5 saturated by the conversion to unsigned, then capped.
+__device__ __forceinline__ float byte_f(uint32_t b) { return __fsub_rn(__uint_as_float(kTwo23Bits | b), kTwo23); }
+
+// Byte k (0..3) of w as a float, exactly.
+__device__ __forceinline__ float byte_of(uint32_t w, int k) {
+  return __fsub_rn(__uint_as_float(__byte_perm(w, kTwo23Bits, 0x7650U | static_cast<uint32_t>(k))), kTwo23);
+}
+
+__device__ __forceinline__ uint32_t floor_bits(float c) { return __float_as_uint(__fadd_rd(c, kTwo23)) - kTwo23Bits; }
+
+// code8 and code16 (below) left in the bits of 2^23 + code: the code in the
+// low byte (low half-word) for packing with byte permutes.
+__device__ __forceinline__ uint32_t code8_bits(float v) {
+  return __float_as_uint(__fadd_rd(fminf(fmaxf(__fadd_rn(v, 0.5F), 0.0F), 255.0F), kTwo23));
+}
+__device__ __forceinline__ uint32_t code16_bits(float v) {
+  return __float_as_uint(__fadd_rd(fminf(fmaxf(__fadd_rn(__fmul_rn(v, 257.0F), 0.5F), 0.0F), 65535.0F), kTwo23));
+}
+// The low bytes of a, b, c, d as one little-endian word.
+__device__ __forceinline__ uint32_t pack8(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  return __byte_perm(__byte_perm(a, b, 0x0040U), __byte_perm(c, d, 0x0040U), 0x5410U);
+}
+// The low half-words of a and b as one little-endian word.
+__device__ __forceinline__ uint32_t pack16(uint32_t a, uint32_t b) { return __byte_perm(a, b, 0x5410U); }
+
+// Rounded half up and clamped to 0..255 (kernel_math.hpp:89-92): r =
+// floor(v + 0.5) then 0 where r <= 0 and 255 where r >= 255 equals the floor
+// of v + 0.5 first clamped to [0, 255].
 __device__ __forceinline__ uint32_t code8(float v) {
-  const uint32_t r = __float2uint_rd(v + 0.5F);
-  return r < 255U ? r : 255U;
+  return floor_bits(fminf(fmaxf(__fadd_rn(v, 0.5F), 0.0F), 255.0F));
 }
 
 // 16-bit codes: the floor of v * 257 + 0.5, clamped to 0..65535 (:94-97).
 __device__ __forceinline__ uint32_t code16(float v) {
-  const float p = v * 257.0F;
-  const uint32_t r = __float2uint_rd(p + 0.5F);
-  return r < 65535U ? r : 65535U;
+  return floor_bits(fminf(fmaxf(__fadd_rn(__fmul_rn(v, 257.0F), 0.5F), 0.0F), 65535.0F));
 }
 
-// A 16-bit little-endian sample on the 8-bit scale (:99-104), read byte-wise
-// since a pitched row of 16-bit samples need not be 2-byte aligned.
+// v / 257 correctly rounded for an integer 0 <= v < 2^16, as the IEEE
+// division the definition uses (:99-104): the product by r = RN(1/257)
+// corrected once by its exact FMA residual (Markstein's correction step),
+// which gives the correctly rounded quotient for every one of the 65,536
+// inputs (checked exhaustively against exact rational arithmetic, and on the
+// GPU against the oracle's division).
+__device__ __forceinline__ float div257(uint32_t v) {
+  constexpr float kR = 1.0F / 257.0F;
+  const float x = byte_f(v);  // exact for v < 2^23
+  const float q = __fmul_rn(x, kR);
+  const float e = __fmaf_rn(-q, 257.0F, x);
+  return __fmaf_rn(e, kR, q);
+}
+
+// A 16-bit little-endian sample on the 8-bit scale, read byte-wise since a
+// pitched row of 16-bit samples need not be 2-byte aligned.
 __device__ __forceinline__ float word_sample(const uint8_t* p) {
-  const uint32_t v = static_cast<uint32_t>(__ldg(p)) | (static_cast<uint32_t>(__ldg(p + 1)) << 8);
-  return __fdiv_rn(static_cast<float>(v), 257.0F);
+  return div257(static_cast<uint32_t>(__ldg(p)) | (static_cast<uint32_t>(__ldg(p + 1)) << 8));
 }
 
 __device__ __forceinline__ const uint8_t* row_of(const Image& img, int plane, int y) {
@@ -139,10 +179,125 @@ __device__ __forceinline__ Px load_px(const Image& img, int x, int y) {
   }
 }
 
+__device__ __forceinline__ bool aligned4(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 3U) == 0U; }
+
+__device__ __forceinline__ uint32_t ldw(const uint8_t* p) { return __ldg(reinterpret_cast<const uint32_t*>(p)); }
+
+// Source pixels sx .. sx + 3 of row sy in two steps, so that a thread can
+// issue all its loads before its arithmetic: fetch4 reads their bytes as
+// whole words (false, reading nothing, where the words would not be 4-byte
+// aligned), decode4 turns the words into the samples load_px gives.
+constexpr int kRawWords = 6;
+
+template <int kF>
+__device__ __forceinline__ bool fetch4(const Image& img, int sx, int sy, uint32_t (&w)[kRawWords]) {
+  const uint8_t* row = row_of(img, 0, sy);
+  if constexpr (kF == CC_RGB8 || kF == CC_BGR8) {
+    const uint8_t* p = row + 3 * sx;
+    if (!aligned4(p)) return false;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) w[k] = ldw(p + 4 * k);
+  } else if constexpr (kF == CC_RGBA8 || kF == CC_BGRA8) {
+    const uint8_t* p = row + 4 * sx;
+    if (!aligned4(p)) return false;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) w[k] = ldw(p + 4 * k);
+  } else if constexpr (kF == CC_MONO8) {
+    const uint8_t* p = row + sx;
+    if (!aligned4(p)) return false;
+    w[0] = ldw(p);
+  } else if constexpr (kF == CC_MONO16) {
+    const uint8_t* p = row + 2 * sx;
+    if (!aligned4(p)) return false;
+    w[0] = ldw(p);
+    w[1] = ldw(p + 4);
+  } else if constexpr (kF == CC_RGB16) {
+    const uint8_t* p = row + 6 * sx;
+    if (!aligned4(p)) return false;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) w[k] = ldw(p + 4 * k);
+  } else if constexpr (kF == CC_NV12 || kF == CC_NV16) {
+    // Four luma bytes and, from an even column, the two chroma pairs covering them.
+    const uint8_t* p = row + sx;
+    const uint8_t* uv = row_of(img, 1, kF == CC_NV12 ? (sy >> 1) : sy) + sx;
+    if ((sx & 1) != 0 || !aligned4(p) || !aligned4(uv)) return false;
+    w[0] = ldw(p);
+    w[1] = ldw(uv);
+  } else if constexpr (kF == CC_I420) {
+    const uint8_t* p = row + sx;
+    if ((sx & 1) != 0 || !aligned4(p)) return false;
+    w[0] = ldw(p);
+    const uint8_t* u = row_of(img, 1, sy >> 1) + (sx >> 1);
+    const uint8_t* v = row_of(img, 2, sy >> 1) + (sx >> 1);
+    // Cb0, Cr0, Cb1, Cr1 as the chroma word of the semi-planar formats.
+    w[1] = static_cast<uint32_t>(__ldg(u)) | (static_cast<uint32_t>(__ldg(v)) << 8) |
+           (static_cast<uint32_t>(__ldg(u + 1)) << 16) | (static_cast<uint32_t>(__ldg(v + 1)) << 24);
+  } else {
+    // YUYV / UYVY: two pixel pairs, one word each, from an even column.
+    const uint8_t* p = row + 2 * sx;
+    if ((sx & 1) != 0 || !aligned4(p)) return false;
+    w[0] = ldw(p);
+    w[1] = ldw(p + 4);
+  }
+  return true;
+}
+
+template <int kF>
+__device__ __forceinline__ void decode4(const uint32_t (&w)[kRawWords], Px (&s)[4]) {
+  if constexpr (kF == CC_RGB8 || kF == CC_BGR8) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float a = byte_of(w[(3 * i) >> 2], (3 * i) & 3);
+      const float b = byte_of(w[(3 * i + 1) >> 2], (3 * i + 1) & 3);
+      const float c = byte_of(w[(3 * i + 2) >> 2], (3 * i + 2) & 3);
+      s[i] = kF == CC_RGB8 ? Px{a, b, c, 255.0F} : Px{c, b, a, 255.0F};
+    }
+  } else if constexpr (kF == CC_RGBA8 || kF == CC_BGRA8) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float a = byte_of(w[i], 0), b = byte_of(w[i], 1), c = byte_of(w[i], 2), al = byte_of(w[i], 3);
+      s[i] = kF == CC_RGBA8 ? Px{a, b, c, al} : Px{c, b, a, al};
+    }
+  } else if constexpr (kF == CC_MONO8) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) s[i] = Px{byte_of(w[0], i), 0.0F, 0.0F, 255.0F};
+  } else if constexpr (kF == CC_MONO16) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) s[i] = Px{div257((w[i >> 1] >> (16 * (i & 1))) & 0xFFFFU), 0.0F, 0.0F, 255.0F};
+  } else if constexpr (kF == CC_RGB16) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      float c[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) c[j] = div257((w[(3 * i + j) >> 1] >> (16 * ((3 * i + j) & 1))) & 0xFFFFU);
+      s[i] = Px{c[0], c[1], c[2], 255.0F};
+    }
+  } else if constexpr (kF == CC_NV12 || kF == CC_NV16 || kF == CC_I420) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      s[i] = Px{byte_of(w[0], i), byte_of(w[1], 2 * (i >> 1)), byte_of(w[1], 2 * (i >> 1) + 1), 255.0F};
+    }
+  } else {
+    constexpr int kY = kF == CC_YUYV ? 0 : 1;  // byte of the first luma in a pair
+    constexpr int kU = kF == CC_YUYV ? 1 : 0;  // byte of Cb; Cr two later
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint32_t q = w[i >> 1];
+      s[i] = Px{byte_of(q, kY + 2 * (i & 1)), byte_of(q, kU), byte_of(q, kU + 2), 255.0F};
+    }
+  }
+}
+
 // c = m s + o on the colour samples, each row summed left to right; alpha
-// passes through (:236-244).
+// passes through (:236-244). kKnown: whether the identity is settled at
+// compile time (kIdentity then says which), else p.identity decides.
+template <bool kKnown = false, bool kIdentity = false>
 __device__ __forceinline__ Px apply_affine(const Plan& p, Px s) {
-  if (p.identity) return s;
+  if constexpr (kKnown) {
+    if constexpr (kIdentity) return s;
+  } else {
+    if (p.identity) return s;
+  }
   Px r;
   r.c0 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p.m[0], s.c0), __fmul_rn(p.m[1], s.c1)), __fmul_rn(p.m[2], s.c2)),
                    p.o[0]);

@@ -89,92 +89,256 @@ __device__ __forceinline__ void store_row4(const Image& img, int x, int y, const
   put_segment<kWords>(row + static_cast<size_t>(x) * kBpp, w, n * kBpp);
 }
 
-// Direct path: thread (gx, gy) converts pixels [4 gx, 4 gx + 4) of rows
-// [gy << bsy, (gy + 1) << bsy).
+// One four-pixel row segment of format kDst at (x, y) from whole, aligned
+// groups: every word of it stored, the row start known to be 4-byte aligned.
+// Codes come as their 2^23-biased bits (code8_bits / code16_bits); cb and cr
+// are the pair chroma of the packed 4:2:2 formats.
+template <int kDst>
+__device__ __forceinline__ void store_full4(const Image& img, int x, int y, const Px (&v)[kGroupX],
+                                            const uint32_t (&cb)[2], const uint32_t (&cr)[2]) {
+  uint8_t* row = img.data[0] + static_cast<size_t>(y) * img.pitch[0];
+  if constexpr (kDst == CC_NV12 || kDst == CC_NV16 || kDst == CC_I420 || kDst == CC_MONO8) {
+    *reinterpret_cast<uint32_t*>(row + x) =
+        pack8(code8_bits(v[0].c0), code8_bits(v[1].c0), code8_bits(v[2].c0), code8_bits(v[3].c0));
+  } else if constexpr (kDst == CC_YUYV || kDst == CC_UYVY) {
+    uint32_t* q = reinterpret_cast<uint32_t*>(row + 2 * x);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const uint32_t y0 = code8_bits(v[2 * k].c0), y1 = code8_bits(v[2 * k + 1].c0);
+      q[k] = kDst == CC_YUYV ? pack8(y0, cb[k], y1, cr[k]) : pack8(cb[k], y0, cr[k], y1);
+    }
+  } else if constexpr (kDst == CC_RGB8 || kDst == CC_BGR8) {
+    const bool bgr = kDst == CC_BGR8;
+    uint32_t b[12];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      b[3 * i] = code8_bits(bgr ? v[i].c2 : v[i].c0);
+      b[3 * i + 1] = code8_bits(v[i].c1);
+      b[3 * i + 2] = code8_bits(bgr ? v[i].c0 : v[i].c2);
+    }
+    uint32_t* q = reinterpret_cast<uint32_t*>(row + 3 * x);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) q[k] = pack8(b[4 * k], b[4 * k + 1], b[4 * k + 2], b[4 * k + 3]);
+  } else if constexpr (kDst == CC_RGBA8 || kDst == CC_BGRA8) {
+    const bool bgr = kDst == CC_BGRA8;
+    uint32_t* q = reinterpret_cast<uint32_t*>(row + 4 * x);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      q[i] = pack8(code8_bits(bgr ? v[i].c2 : v[i].c0), code8_bits(v[i].c1), code8_bits(bgr ? v[i].c0 : v[i].c2),
+                   code8_bits(v[i].a));
+    }
+  } else if constexpr (kDst == CC_MONO16) {
+    uint32_t* q = reinterpret_cast<uint32_t*>(row + 2 * x);
+    q[0] = pack16(code16_bits(v[0].c0), code16_bits(v[1].c0));
+    q[1] = pack16(code16_bits(v[2].c0), code16_bits(v[3].c0));
+  } else {
+    uint32_t h[12];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      h[3 * i] = code16_bits(v[i].c0);
+      h[3 * i + 1] = code16_bits(v[i].c1);
+      h[3 * i + 2] = code16_bits(v[i].c2);
+    }
+    uint32_t* q = reinterpret_cast<uint32_t*>(row + 6 * x);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) q[k] = pack16(h[2 * k], h[2 * k + 1]);
+  }
+}
+
+// Four-pixel subgroups a direct-path thread takes across: two for a 4:2:0
+// destination (whose thread also takes two rows), four otherwise, so that
+// each thread has a few dozen bytes of loads in flight.
+__host__ __device__ constexpr int direct_subgroups(int dst) {
+  return (dst == CC_NV12 || dst == CC_I420) ? 2 : 4;
+}
+
+// Direct path: a warp converts kSub x 32 four-pixel groups of rows
+// [gy << bsy, (gy + 1) << bsy); its lane L takes groups g0 + 32 h (h < kSub),
+// so that every load and store instruction of the warp covers contiguous
+// bytes. All of a thread's whole, aligned source groups are read first
+// (fetch4); then each group is converted and stored; pixels outside the
+// content take the fill, and groups that are partial or unaligned read pixel
+// by pixel. groups_x = ceil(width / 4).
 template <int kSrc, int kDst>
 __global__ void __launch_bounds__(kThreadsX* kThreadsY) cc_direct_kernel(const __grid_constant__ Plan p, int groups_x,
                                                                          int groups_y) {
-  const int gx = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
   const int gy = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
-  if (gx >= groups_x || gy >= groups_y) return;
+  if (gy >= groups_y) return;
   constexpr FormatInfo fi = info_of(kDst);
   constexpr bool kYuvDst = fi.model == kYuv;
   constexpr int kRows = kYuvDst ? (1 << fi.shift_y) : 1;
-  const int x0 = gx * kGroupX;
+  constexpr int kSub = direct_subgroups(kDst);
+  const int g0 = static_cast<int>(blockIdx.x) * kThreadsX * kSub + static_cast<int>(threadIdx.x);
+  if (g0 >= groups_x) return;
   const int y0 = gy * kRows;
-  const int n = p.dst.width - x0 < kGroupX ? p.dst.width - x0 : kGroupX;
   // Source offset of destination pixel (x, y) inside the content.
   const int ox = p.sx0 - p.cx0;
   const int oy = p.sy0 - p.cy0;
-  float cbs[2] = {0.0F, 0.0F}, crs[2] = {0.0F, 0.0F};
-  int rows = 0;
+
+  uint32_t raw[kRows][kSub][kRawWords];
+  bool ok[kRows][kSub];
 #pragma unroll
   for (int r = 0; r < kRows; ++r) {
     const int y = y0 + r;
-    if (r > 0 && y >= p.dst.height) break;
-    ++rows;
-    Px v[kGroupX];
-    const bool row_in = y >= p.cy0 && y < p.cy1;
+    const bool row_in = (r == 0 || y < p.dst.height) && y >= p.cy0 && y < p.cy1;
 #pragma unroll
-    for (int i = 0; i < kGroupX; ++i) {
-      const int x = x0 + i;
-      if (i < n && row_in && x >= p.cx0 && x < p.cx1) {
-        v[i] = apply_affine(p, load_px<kSrc>(p.src, x + ox, y + oy));
-      } else {
-        v[i] = Px{p.fill[0], p.fill[1], p.fill[2], p.fill[3]};
-      }
-      if constexpr (kYuvDst) {
-        if (i < n) {
-          cbs[i >> 1] = __fadd_rn(cbs[i >> 1], v[i].c1);
-          crs[i >> 1] = __fadd_rn(crs[i >> 1], v[i].c2);
-        }
-      }
-    }
-    if constexpr (kDst == CC_YUYV || kDst == CC_UYVY) {
-      // One row per block: the chroma of each pixel pair is known now.
-      uint32_t cb[2], cr[2];
-#pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        const float cnt = n - 2 * b >= 2 ? 2.0F : 1.0F;
-        cb[b] = code8(__fdiv_rn(cbs[b], cnt));
-        cr[b] = code8(__fdiv_rn(crs[b], cnt));
-      }
-      store_row4<kDst>(p.dst, x0, y, v, n, cb, cr);
-    } else {
-      const uint32_t none[2] = {0U, 0U};
-      store_row4<kDst>(p.dst, x0, y, v, n, none, none);
+    for (int h = 0; h < kSub; ++h) {
+      const int xs = (g0 + kThreadsX * h) * kGroupX;
+      ok[r][h] = row_in && xs + kGroupX <= p.dst.width && xs >= p.cx0 && xs + kGroupX <= p.cx1 &&
+                 fetch4<kSrc>(p.src, xs + ox, y + oy, raw[r][h]);
     }
   }
-  if constexpr (kDst == CC_NV12 || kDst == CC_NV16 || kDst == CC_I420) {
-    const int cx = x0 >> 1;
-    const int cy = y0 >> fi.shift_y;
-    const int nb = (n + 1) >> 1;  // chroma samples in this group: 1 or 2
-    uint32_t code[2][2];
+
+  // Interior fast path: every group fetched (so whole, inside the content
+  // and the frame, rows included) and every destination row it writes
+  // 4-byte aligned (2-byte for the I420 chroma planes): no per-pixel checks.
+  bool full = true;
 #pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      const int cols = n - 2 * b >= 2 ? 2 : 1;
-      const float cnt = static_cast<float>(cols * rows);
-      code[b][0] = code8(__fdiv_rn(cbs[b], cnt));
-      code[b][1] = code8(__fdiv_rn(crs[b], cnt));
-    }
-    if constexpr (kDst == CC_I420) {
-      uint8_t* u = p.dst.data[1] + static_cast<size_t>(cy) * p.dst.pitch[1] + cx;
-      uint8_t* vv = p.dst.data[2] + static_cast<size_t>(cy) * p.dst.pitch[2] + cx;
-      const uint32_t uw[1] = {code[0][0] | (code[1][0] << 8)};
-      const uint32_t vw[1] = {code[0][1] | (code[1][1] << 8)};
-      if (nb == 2 && (reinterpret_cast<uintptr_t>(u) & 1U) == 0U && (reinterpret_cast<uintptr_t>(vv) & 1U) == 0U) {
-        *reinterpret_cast<uint16_t*>(u) = static_cast<uint16_t>(uw[0]);
-        *reinterpret_cast<uint16_t*>(vv) = static_cast<uint16_t>(vw[0]);
-      } else {
-        for (int b = 0; b < nb; ++b) {
-          u[b] = static_cast<uint8_t>(code[b][0]);
-          vv[b] = static_cast<uint8_t>(code[b][1]);
+  for (int r = 0; r < kRows; ++r) {
+#pragma unroll
+    for (int h = 0; h < kSub; ++h) full = full && ok[r][h];
+    full = full && aligned4(row_of(p.dst, 0, y0 + r));
+  }
+  if constexpr (kDst == CC_NV12 || kDst == CC_NV16) {
+    full = full && aligned4(row_of(p.dst, 1, y0 >> fi.shift_y));
+  } else if constexpr (kDst == CC_I420) {
+    full = full && ((reinterpret_cast<uintptr_t>(row_of(p.dst, 1, y0 >> 1)) |
+                     reinterpret_cast<uintptr_t>(row_of(p.dst, 2, y0 >> 1))) & 1U) == 0U;
+  }
+  if (full) {
+    constexpr bool kIdentity = info_of(kSrc).model == fi.model;
+#pragma unroll
+    for (int h = 0; h < kSub; ++h) {
+      const int xs = (g0 + kThreadsX * h) * kGroupX;
+      float cbs[2] = {0.0F, 0.0F}, crs[2] = {0.0F, 0.0F};
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        Px v[kGroupX];
+        decode4<kSrc>(raw[r][h], v);
+#pragma unroll
+        for (int i = 0; i < kGroupX; ++i) {
+          v[i] = apply_affine<true, kIdentity>(p, v[i]);
+          if constexpr (kYuvDst) {
+            cbs[i >> 1] = __fadd_rn(cbs[i >> 1], v[i].c1);
+            crs[i >> 1] = __fadd_rn(crs[i >> 1], v[i].c2);
+          }
+        }
+        uint32_t cb[2] = {0U, 0U}, cr[2] = {0U, 0U};
+        if constexpr (kDst == CC_YUYV || kDst == CC_UYVY) {
+#pragma unroll
+          for (int b = 0; b < 2; ++b) {
+            cb[b] = code8_bits(__fmul_rn(cbs[b], 0.5F));
+            cr[b] = code8_bits(__fmul_rn(crs[b], 0.5F));
+          }
+        }
+        store_full4<kDst>(p.dst, xs, y0 + r, v, cb, cr);
+      }
+      if constexpr (kDst == CC_NV12 || kDst == CC_NV16 || kDst == CC_I420) {
+        constexpr float kInv = kRows == 2 ? 0.25F : 0.5F;  // 2 x kRows pixels a block
+        const uint32_t b0 = code8_bits(__fmul_rn(cbs[0], kInv)), r0 = code8_bits(__fmul_rn(crs[0], kInv));
+        const uint32_t b1 = code8_bits(__fmul_rn(cbs[1], kInv)), r1 = code8_bits(__fmul_rn(crs[1], kInv));
+        const int cy = y0 >> fi.shift_y;
+        if constexpr (kDst == CC_I420) {
+          *reinterpret_cast<uint16_t*>(p.dst.data[1] + static_cast<size_t>(cy) * p.dst.pitch[1] + (xs >> 1)) =
+              static_cast<uint16_t>(__byte_perm(b0, b1, 0x0040U));
+          *reinterpret_cast<uint16_t*>(p.dst.data[2] + static_cast<size_t>(cy) * p.dst.pitch[2] + (xs >> 1)) =
+              static_cast<uint16_t>(__byte_perm(r0, r1, 0x0040U));
+        } else {
+          *reinterpret_cast<uint32_t*>(p.dst.data[1] + static_cast<size_t>(cy) * p.dst.pitch[1] + xs) =
+              pack8(b0, r0, b1, r1);
         }
       }
-    } else {
-      uint8_t* q = p.dst.data[1] + static_cast<size_t>(cy) * p.dst.pitch[1] + 2 * cx;
-      const uint32_t w[1] = {code[0][0] | (code[0][1] << 8) | (code[1][0] << 16) | (code[1][1] << 24)};
-      put_segment<1>(q, w, 2 * nb);
+    }
+    return;
+  }
+
+#pragma unroll
+  for (int h = 0; h < kSub; ++h) {
+    const int xs = (g0 + kThreadsX * h) * kGroupX;
+    if (xs >= p.dst.width) break;  // later groups lie further right
+    const int n = p.dst.width - xs < kGroupX ? p.dst.width - xs : kGroupX;
+    float cbs[2] = {0.0F, 0.0F}, crs[2] = {0.0F, 0.0F};
+    int rows = 0;
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const int y = y0 + r;
+      if (r > 0 && y >= p.dst.height) break;
+      ++rows;
+      Px v[kGroupX];
+      if (ok[r][h]) {
+        decode4<kSrc>(raw[r][h], v);
+#pragma unroll
+        for (int i = 0; i < kGroupX; ++i) v[i] = apply_affine(p, v[i]);
+      } else {
+        const bool row_in = y >= p.cy0 && y < p.cy1;
+#pragma unroll
+        for (int i = 0; i < kGroupX; ++i) {
+          const int x = xs + i;
+          if (i < n && row_in && x >= p.cx0 && x < p.cx1) {
+            v[i] = apply_affine(p, load_px<kSrc>(p.src, x + ox, y + oy));
+          } else {
+            v[i] = Px{p.fill[0], p.fill[1], p.fill[2], p.fill[3]};
+          }
+        }
+      }
+      if constexpr (kYuvDst) {
+#pragma unroll
+        for (int i = 0; i < kGroupX; ++i) {
+          if (i < n) {
+            cbs[i >> 1] = __fadd_rn(cbs[i >> 1], v[i].c1);
+            crs[i >> 1] = __fadd_rn(crs[i >> 1], v[i].c2);
+          }
+        }
+      }
+      // Chroma means: a block holds 1, 2 or 4 pixels, and a sum of these
+      // samples is zero or far above the subnormals, so dividing by the count
+      // (as the definition does) is exactly the product by its reciprocal.
+      if constexpr (kDst == CC_YUYV || kDst == CC_UYVY) {
+        // One row per block: the chroma of each pixel pair is known now.
+        uint32_t cb[2], cr[2];
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          const float inv = n - 2 * b >= 2 ? 0.5F : 1.0F;
+          cb[b] = code8(__fmul_rn(cbs[b], inv));
+          cr[b] = code8(__fmul_rn(crs[b], inv));
+        }
+        store_row4<kDst>(p.dst, xs, y, v, n, cb, cr);
+      } else {
+        const uint32_t none[2] = {0U, 0U};
+        store_row4<kDst>(p.dst, xs, y, v, n, none, none);
+      }
+    }
+    if constexpr (kDst == CC_NV12 || kDst == CC_NV16 || kDst == CC_I420) {
+      const int cx = xs >> 1;
+      const int cy = y0 >> fi.shift_y;
+      const int nb = (n + 1) >> 1;  // chroma samples in this subgroup: 1 or 2
+      uint32_t code[2][2];
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const int cnt = (n - 2 * b >= 2 ? 2 : 1) * rows;
+        const float inv = cnt == 4 ? 0.25F : (cnt == 2 ? 0.5F : 1.0F);
+        code[b][0] = code8(__fmul_rn(cbs[b], inv));
+        code[b][1] = code8(__fmul_rn(crs[b], inv));
+      }
+      if constexpr (kDst == CC_I420) {
+        uint8_t* u = p.dst.data[1] + static_cast<size_t>(cy) * p.dst.pitch[1] + cx;
+        uint8_t* vv = p.dst.data[2] + static_cast<size_t>(cy) * p.dst.pitch[2] + cx;
+        if (nb == 2 && (reinterpret_cast<uintptr_t>(u) & 1U) == 0U && (reinterpret_cast<uintptr_t>(vv) & 1U) == 0U) {
+          *reinterpret_cast<uint16_t*>(u) = static_cast<uint16_t>(code[0][0] | (code[1][0] << 8));
+          *reinterpret_cast<uint16_t*>(vv) = static_cast<uint16_t>(code[0][1] | (code[1][1] << 8));
+        } else {
+          u[0] = static_cast<uint8_t>(code[0][0]);
+          vv[0] = static_cast<uint8_t>(code[0][1]);
+          if (nb == 2) {
+            u[1] = static_cast<uint8_t>(code[1][0]);
+            vv[1] = static_cast<uint8_t>(code[1][1]);
+          }
+        }
+      } else {
+        uint8_t* q = p.dst.data[1] + static_cast<size_t>(cy) * p.dst.pitch[1] + 2 * cx;
+        const uint32_t w[1] = {code[0][0] | (code[0][1] << 8) | (code[1][0] << 16) | (code[1][1] << 24)};
+        put_segment<1>(q, w, 2 * nb);
+      }
     }
   }
 }

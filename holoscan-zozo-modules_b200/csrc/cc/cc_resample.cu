@@ -90,21 +90,24 @@ int launch_convert(const Plan& plan, void* stream) {
   const dim3 block(kThreadsX, kThreadsY);
   Plan p = plan;
   const bool direct = direct_path(p);
-  int across, down;
+  int across, down, per_block_x;
   const void* fn;
   if (direct) {
+    // Four-pixel groups across; a block's warp covers kSub x 32 of them.
     const FormatInfo fi = info_of(p.dst.format);
     const int rows = fi.model == kYuv ? (1 << fi.shift_y) : 1;
     across = (p.dst.width + kGroupX - 1) / kGroupX;
     down = (p.dst.height + rows - 1) / rows;
+    per_block_x = kThreadsX * direct_subgroups(p.dst.format);
     fn = direct_kernel(p.src.format, p.dst.format);
   } else {
     across = (p.dst.width + (1 << p.bsx) - 1) >> p.bsx;
     down = (p.dst.height + (1 << p.bsy) - 1) >> p.bsy;
+    per_block_x = kThreadsX;
     fn = resample_kernel(p.src.format, p.mode);
   }
   if (fn == nullptr || (down + kThreadsY - 1) / kThreadsY > 65535) return static_cast<int>(cudaErrorInvalidValue);
-  const dim3 grid(static_cast<unsigned>((across + kThreadsX - 1) / kThreadsX),
+  const dim3 grid(static_cast<unsigned>((across + per_block_x - 1) / per_block_x),
                   static_cast<unsigned>((down + kThreadsY - 1) / kThreadsY));
   void* args[] = {&p, &across, &down};
   return static_cast<int>(cudaLaunchKernel(fn, grid, block, args, 0, static_cast<cudaStream_t>(stream)));

@@ -132,7 +132,7 @@ def test_direct_path_with_border_crop_and_upscale():
     for src in (cc.NV12, cc.UYVY, cc.RGB8, cc.BGRA8, cc.MONO16, cc.RGB16, cc.I420):
         img = occ.noise(src, 40, 22, 11)
         for dst in cc.ALL_FORMATS:
-            for dw, dh, crop, box in ((40, 40, None, True), (60, 22, None, True), (26, 15, (7, 3, 26, 15), False),
+            for dw, dh, crop, box in ((40, 40, None, True), (60, 22, None, True), (26, 15, (7, 3, 26, 15), False), (24, 15, (8, 2, 24, 15), False),
                                       (80, 47, None, False), (22, 40, (9, 0, 22, 22), True)):
                 if needs_even_width(dst) and dw % 2:
                     continue
@@ -167,6 +167,23 @@ def test_pitched_nv12_as_the_reference_test():
     (converter_test.cpp:195-227)."""
     img = occ.noise(cc.NV12, 50, 20, 9)
     assert expect_same(img, cc.NV12, 50, 20, cc.RGBA8, 40, 16, cc.params(mode=cc.BILINEAR), pads=(14, 96)) == 0
+
+
+def test_every_16bit_sample():
+    """All 65,536 16-bit values, as MONO16 and RGB16 sources, through the
+    direct and the resample paths: the kernels' division by 257 is the
+    correctly rounded one for every input."""
+    values = np.arange(65536, dtype=np.uint16)
+    mono = values.view(np.uint8).copy()  # 256x256, little-endian
+    rgb16 = np.stack([values, values[::-1], np.roll(values, 12345)], axis=1).reshape(-1).view(np.uint8).copy()
+    bad = []
+    for src, img in ((cc.MONO16, mono), (cc.RGB16, rgb16)):
+        for dst in (cc.MONO16, cc.RGB16, cc.RGB8, cc.NV12):
+            for dw, dh, mode in ((256, 256, cc.NEAREST), (255, 129, cc.BILINEAR), (100, 37, cc.AREA)):
+                wrong = expect_same(img, src, 256, 256, dst, dw, dh, cc.params(cc.BT601, cc.FULL, mode))
+                if wrong:
+                    bad.append((NAMES[src], NAMES[dst], dw, dh, mode, wrong))
+    assert not bad, bad
 
 
 def test_golden_fixtures():
