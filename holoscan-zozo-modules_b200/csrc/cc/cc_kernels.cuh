@@ -13,6 +13,7 @@
 // compile time, the destination's stores chosen at run time.
 #pragma once
 
+#include "../isp_ops.cuh"
 #include "cc_common.cuh"
 
 namespace cc_b200 {
@@ -87,6 +88,34 @@ __device__ __forceinline__ void store_row4(const Image& img, int x, int y, const
     }
   }
   put_segment<kWords>(row + static_cast<size_t>(x) * kBpp, w, n * kBpp);
+}
+
+// The colour map of two pixels at once: the nine products two lanes at a
+// time (mul.rn.f32x2, each lane rounded as the scalar product), every sum per
+// lane in the definition's order; a two-lane product never feeds a two-lane
+// sum, which the assembler could fuse into one rounding.
+template <bool kIdentity>
+__device__ __forceinline__ void affine_pair(const Plan& p, Px& a, Px& b) {
+  if constexpr (!kIdentity) {
+    using isp_b200::add_lanes;
+    using isp_b200::bc2;
+    using isp_b200::mul2;
+    const float2 s0 = make_float2(a.c0, b.c0), s1 = make_float2(a.c1, b.c1), s2 = make_float2(a.c2, b.c2);
+    float2 out[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float2 t0 = mul2(bc2(p.m[3 * k]), s0);
+      const float2 t1 = mul2(bc2(p.m[3 * k + 1]), s1);
+      const float2 t2 = mul2(bc2(p.m[3 * k + 2]), s2);
+      out[k] = add_lanes(add_lanes(add_lanes(t0, t1), t2), bc2(p.o[k]));
+    }
+    a.c0 = out[0].x;
+    b.c0 = out[0].y;
+    a.c1 = out[1].x;
+    b.c1 = out[1].y;
+    a.c2 = out[2].x;
+    b.c2 = out[2].y;
+  }
 }
 
 // One four-pixel row segment of format kDst at (x, y) from whole, aligned
@@ -215,9 +244,10 @@ __global__ void __launch_bounds__(kThreadsX* kThreadsY) cc_direct_kernel(const _
       for (int r = 0; r < kRows; ++r) {
         Px v[kGroupX];
         decode4<kSrc>(raw[r][h], v);
+        affine_pair<kIdentity>(p, v[0], v[1]);
+        affine_pair<kIdentity>(p, v[2], v[3]);
 #pragma unroll
         for (int i = 0; i < kGroupX; ++i) {
-          v[i] = apply_affine<true, kIdentity>(p, v[i]);
           if constexpr (kYuvDst) {
             cbs[i >> 1] = __fadd_rn(cbs[i >> 1], v[i].c1);
             crs[i >> 1] = __fadd_rn(crs[i >> 1], v[i].c2);
