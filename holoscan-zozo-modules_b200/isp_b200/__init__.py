@@ -100,6 +100,8 @@ def lib() -> C.CDLL:
         L.isp_b200_synth_default.restype = None
         L.isp_b200_synthetic_raw.argtypes = [P(abi.SynthC), C.c_uint64, C.c_void_p, C.c_size_t, C.c_void_p]
         L.isp_b200_server_destroy.argtypes = [C.c_void_p]
+        L.isp_b200_view_compose.argtypes = [P(abi.RawViewC), C.c_float, C.c_void_p, C.c_size_t, C.c_void_p,
+                                            C.c_size_t, C.c_void_p]
         if L.isp_b200_abi_version() != abi.ABI_VERSION:
             raise RuntimeError("libisp_b200.so ABI version mismatch")
         _lib = L
@@ -379,6 +381,14 @@ def process_noalloc(params: IspParams, raw: abi.RawViewC, out: abi.RgbViewC, his
     exp = abi.ExposureC(exposure[0], exposure[1])
     check(lib().isp_b200_process_noalloc(h.ref(), C.byref(raw), C.byref(out), C.byref(st), C.byref(exp),
                                          stream or None))
+
+
+def view_compose(raw: abi.RawViewC, black_level: float, rgb8_ptr: int, rgb8_pitch: int, view_ptr: int,
+                 view_pitch: int, stream: int = 0) -> None:
+    """The demo's side-by-side view (isp_b200_view_compose): device raw frame
+    and RGB8 image in, double-width RGB8 image out, queued on `stream`."""
+    check(lib().isp_b200_view_compose(C.byref(raw), black_level, C.c_void_p(rgb8_ptr), rgb8_pitch,
+                                      C.c_void_p(view_ptr), view_pitch, C.c_void_p(stream)))
 
 
 def params_default() -> abi.ParamsC:

@@ -377,6 +377,18 @@ ISP_B200_API void isp_b200_synth_default(isp_synth_c* config);
 ISP_B200_API int isp_b200_synthetic_raw(const isp_synth_c* config, uint64_t seed, void* raw, size_t pitch,
                            void* stream);
 
+/* The demo's side-by-side view (applications/isp/src/view_op.cu:35-75 and
+ * :143-150), as a headless device image: `view` (RGB8, 2 * raw->width pixels
+ * wide, raw->height rows, row stride view_pitch) gets on its left the raw
+ * mosaic as gray, g = (uint8)(sqrtf(clamp((s - black_level) * scale, 0, 1))
+ * * 255 + 0.5) with scale = 1 / (2^bit_depth - 1 - black_level), each step a
+ * single-precision operation as the demo's kernel does it, and on its right
+ * the ISP's RGB8 image `rgb8` (row stride rgb8_pitch). Device buffers, queued
+ * on stream. ISP_EINVAL for an unusable raw view (as validate_raw: sizes,
+ * format, bit depth, pitch), a missing buffer or a pitch shorter than its row. */
+ISP_B200_API int isp_b200_view_compose(const isp_raw_view_c* raw, float black_level, const void* rgb8,
+                                       size_t rgb8_pitch, void* view, size_t view_pitch, void* stream);
+
 /* One frame without allocating memory. No reference counterpart: for callers
  * that cannot allocate device memory (cudaMalloc forbidden or unsafe where
  * they run, e.g. a host that owns every allocation or a real-time loop that

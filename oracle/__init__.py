@@ -58,8 +58,22 @@ def _lib_oracle():
         lib.oracle_awb_stats.argtypes = [P(abi.ParamsC), P(abi.RawViewC), C.c_void_p]
         lib.oracle_process.argtypes = [P(abi.ParamsC), P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
                                        P(abi.ExposureC), C.c_void_p]
+        lib.oracle_view_compose.argtypes = [P(abi.RawViewC), C.c_float, C.c_void_p, C.c_size_t, C.c_void_p,
+                                            C.c_size_t]
+        lib.oracle_view_compose.restype = None
         _oracle = lib
     return _oracle
+
+
+def view_compose(raw: abi.RawFrame, black: float, rgb: np.ndarray) -> np.ndarray:
+    """The demo's side-by-side view from the C oracle: [H, 2W, 3] uint8 from a
+    raw frame and an [H, W, 3] RGB8 image."""
+    rgb = np.ascontiguousarray(rgb, np.uint8)
+    out = np.zeros((raw.height, 2 * raw.width, 3), np.uint8)
+    rv = raw.view()
+    _lib_oracle().oracle_view_compose(C.byref(rv), black, rgb.ctypes.data, rgb.strides[0], out.ctypes.data,
+                                      out.strides[0])
+    return out
 
 
 def reference_available() -> bool:

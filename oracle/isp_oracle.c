@@ -677,3 +677,33 @@ int oracle_process(const isp_params_c* params, const isp_raw_view_c* raw, const 
   free(lut);
   return ISP_OK;
 }
+
+/* The demo's side-by-side view (applications/isp/src/view_op.cu:35-75,
+ * :143-150), restated: left half the raw mosaic as gray, g =
+ * (uint8)(sqrtf(clamp((s - black) * scale, 0, 1)) * 255 + 0.5) with scale =
+ * 1 / (2^bits - 1 - black) in single precision; right half the RGB8 image.
+ * Host buffers. Parity unpinned: the demo's source needs the Holoscan SDK to
+ * compile, so the reference kernel cannot be run here. */
+void oracle_view_compose(const isp_raw_view_c* raw, float black, const uint8_t* rgb, size_t rgb_pitch, uint8_t* out,
+                         size_t out_pitch) {
+  frame p;
+  memset(&p, 0, sizeof p);
+  p.raw = (const unsigned char*)raw->data;
+  p.raw_pitch = raw->pitch;
+  p.raw_format = raw->format;
+  const float white = (float)((1u << (unsigned)raw->bit_depth) - 1u);
+  const float scale = 1.0F / (white - black);
+  for (int y = 0; y < raw->height; ++y) {
+    uint8_t* o = out + (size_t)y * out_pitch;
+    const uint8_t* i = rgb + (size_t)y * rgb_pitch;
+    for (int x = 0; x < raw->width; ++x) {
+      float v = ((float)load_raw(&p, x, y) - black) * scale;
+      v = v < 0.0F ? 0.0F : v > 1.0F ? 1.0F : v;
+      const uint8_t g = (uint8_t)(sqrtf(v) * 255.0F + 0.5F);
+      o[3 * x] = o[3 * x + 1] = o[3 * x + 2] = g;
+      o[3 * (raw->width + x)] = i[3 * x];
+      o[3 * (raw->width + x) + 1] = i[3 * x + 1];
+      o[3 * (raw->width + x) + 2] = i[3 * x + 2];
+    }
+  }
+}

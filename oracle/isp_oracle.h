@@ -55,6 +55,10 @@ int oracle_process(const isp_params_c* params, const isp_raw_view_c* raw,
                    const isp_rgb_view_c* out, const isp_stats_c* stats,
                    const isp_exposure_c* exposure, oracle_awb_state* state);
 
+/* The demo's side-by-side view of raw and RGB8 (host buffers). */
+void oracle_view_compose(const isp_raw_view_c* raw, float black, const uint8_t* rgb, size_t rgb_pitch, uint8_t* out,
+                         size_t out_pitch);
+
 #ifdef __cplusplus
 }
 #endif
