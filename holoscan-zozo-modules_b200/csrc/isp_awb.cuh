@@ -69,14 +69,21 @@ __device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box,
       }
     }
     // Linear values before white balance, capped at 4 (isp_math.hpp:320-330).
-    float v[2][4];
+    // The two quads of the unit run as the two lanes of f32x2 instructions:
+    // lane x holds sample j of quad 0, lane y sample j of quad 1 (columns
+    // 4u + j and 4u + j + 2, the same Bayer colour). The products feed only a
+    // multiply, a clamp, a per-lane sum or an exact power-of-two scale
+    // (isp_ops.cuh).
+    float2 v[2][2];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       const unsigned int* s = r == 0 ? top : bot;
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int q = (r << 1) | (k & 1);
-        v[r][k] = fmaxf(fmul(fsub(magic_to_float(s[k] | kTwo23Bits), black[q]), inv[q]), 0.0F);
+      for (int j = 0; j < 2; ++j) {
+        const int q = (r << 1) | j;
+        const float2 lin = mul2(sub2(magic_to_float2(s[j] | kTwo23Bits, s[j + 2] | kTwo23Bits), bc2(black[q])),
+                                bc2(inv[q]));
+        v[r][j] = make_float2(fmaxf(lin.x, 0.0F), fmaxf(lin.y, 0.0F));
       }
     }
     if (lt.rows > 0) {
@@ -85,44 +92,49 @@ __device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box,
         for (int r = 0; r < 2; ++r) {
           const int rj = 2 * a + r;
           const int kk = row_k[rj];
-          const float tyj = row_ty[rj];
+          const float2 tyj = bc2(row_ty[rj]);
           const int pl = p.lsc_channels == 4 ? r : 0;
           const float4 t0 = *reinterpret_cast<const float4*>(table + (kk * 2 + pl) * kSW + 4 * u);
           const float4 t1 = *reinterpret_cast<const float4*>(table + ((kk + 1) * 2 + pl) * kSW + 4 * u);
-          v[r][0] = fmul(v[r][0], fadd(t0.x, fmul(fsub(t1.x, t0.x), tyj)));
-          v[r][1] = fmul(v[r][1], fadd(t0.y, fmul(fsub(t1.y, t0.y), tyj)));
-          v[r][2] = fmul(v[r][2], fadd(t0.z, fmul(fsub(t1.z, t0.z), tyj)));
-          v[r][3] = fmul(v[r][3], fadd(t0.w, fmul(fsub(t1.w, t0.w), tyj)));
+          // gain = t0 + (t1 - t0) ty per column (lens_shading_gain, isp_math.hpp:121-140).
+          const float2 a0 = make_float2(t0.x, t0.z), a1 = make_float2(t0.y, t0.w);
+          const float2 g0 = add_lanes(a0, mul2(sub2(make_float2(t1.x, t1.z), a0), tyj));
+          const float2 g1 = add_lanes(a1, mul2(sub2(make_float2(t1.y, t1.w), a1), tyj));
+          v[r][0] = mul2(v[r][0], g0);
+          v[r][1] = mul2(v[r][1], g1);
         }
       } else {
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            v[r][k] = fmul(v[r][k], lens_shading_gain(p, p.lsc, x0 + 4 * u + k, y0 + 2 * a + r,
-                                                      cfa_of(kPat, (r << 1) | (k & 1))));
+          for (int j = 0; j < 2; ++j) {
+            const int channel = cfa_of(kPat, (r << 1) | j);
+            const float gx = lens_shading_gain(p, p.lsc, x0 + 4 * u + j, y0 + 2 * a + r, channel);
+            const float gy = lens_shading_gain(p, p.lsc, x0 + 4 * u + j + 2, y0 + 2 * a + r, channel);
+            v[r][j] = mul2(v[r][j], make_float2(gx, gy));
           }
         }
       }
     }
+    // The quad test per lane: no sample at or above white (isp_math.hpp:316-318).
+    const bool ok0 = qx0 < quads_x && top[0] < white && top[1] < white && bot[0] < white && bot[1] < white;
+    const bool ok1 = qx0 + 1 < quads_x && top[2] < white && top[3] < white && bot[2] < white && bot[3] < white;
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      // A quad with a sample at or above white counts for nothing (isp_math.hpp:316-318).
-      const bool ok = qx0 + q < quads_x && top[2 * q] < white && top[2 * q + 1] < white && bot[2 * q] < white &&
-                      bot[2 * q + 1] < white;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int r = k >> 1;
-        const float x = fminf(v[r][2 * q + (k & 1)], 4.0F);
-        const unsigned int fixed = magic_int(magic_trunc(fadd(fmul(x, kFixedOne), 0.5F)));
-        sum[color_of(cfa_of(kPat, k))] += ok ? fixed : 0U;
-        if constexpr (kWhitePatch) {
-          const unsigned int bin = magic_int(magic_trunc(fmul(x, static_cast<float>(kAwbBins))));
-          if (ok) atomicAdd(&hist[color_of(cfa_of(kPat, k)) * kAwbBins + (bin < kAwbBins - 1 ? bin : kAwbBins - 1)], 1U);
-        }
+    for (int k = 0; k < 4; ++k) {
+      const float2 x = make_float2(fminf(v[k >> 1][k & 1].x, 4.0F), fminf(v[k >> 1][k & 1].y, 4.0F));
+      // to_fixed: trunc(x 2^20 + 0.5), the product exact.
+      const float2 m = magic_trunc2(exact_scale_add2(x, bc2(kFixedOne), bc2(0.5F)));
+      sum[color_of(cfa_of(kPat, k))] += (ok0 ? magic_int(m.x) : 0U) + (ok1 ? magic_int(m.y) : 0U);
+      if constexpr (kWhitePatch) {
+        // trunc(x 1024): an exact product, so its two-lane truncation is safe.
+        const float2 b = magic_trunc2(mul2(x, bc2(static_cast<float>(kAwbBins))));
+        const unsigned int b0 = magic_int(b.x), b1 = magic_int(b.y);
+        unsigned int* h = hist + color_of(cfa_of(kPat, k)) * kAwbBins;
+        if (ok0) atomicAdd(&h[b0 < kAwbBins - 1 ? b0 : kAwbBins - 1], 1U);
+        if (ok1) atomicAdd(&h[b1 < kAwbBins - 1 ? b1 : kAwbBins - 1], 1U);
       }
-      quads += ok ? 1U : 0U;
     }
+    quads += (ok0 ? 1U : 0U) + (ok1 ? 1U : 0U);
   }
 }
 
