@@ -341,11 +341,6 @@ def run_b200(args):
     with torch.cuda.stream(stream):
         for i in range(args.warmup):
             step(i)
-        # Per-step events around the fused tile kernel (the roofline's kernel).
-        before = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        after = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        for e in before + after:
-            e.record(stream)  # creates the CUDA event behind the handle
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
         clocks = Clocks(local)
@@ -354,14 +349,25 @@ def run_b200(args):
         barrier()
         start.record(stream)
         for i in range(args.steps):
-            L.isp_b200_set_kernel_events(pipe.handle, C.c_void_p(before[i].cuda_event), C.c_void_p(after[i].cuda_event))
             step(i)
         end.record(stream)
-        L.isp_b200_set_kernel_events(pipe.handle, None, None)
         barrier()
         clock_info = clocks.stop()
+        # The fused tile kernel alone (the roofline's kernel): events recorded
+        # around it in a second run of steps. They keep it from overlapping
+        # the statistics pass, so this is its own duration.
+        ksteps = min(args.steps, 400)
+        before = [torch.cuda.Event(enable_timing=True) for _ in range(ksteps)]
+        after = [torch.cuda.Event(enable_timing=True) for _ in range(ksteps)]
+        for e in before + after:
+            e.record(stream)  # creates the CUDA event behind the handle
+        for i in range(ksteps):
+            L.isp_b200_set_kernel_events(pipe.handle, C.c_void_p(before[i].cuda_event), C.c_void_p(after[i].cuda_event))
+            step(i)
+        L.isp_b200_set_kernel_events(pipe.handle, None, None)
+        torch.cuda.synchronize()
     elapsed_ms = start.elapsed_time(end)
-    kernel_ms = sum(b.elapsed_time(a) for b, a in zip(before, after)) / args.steps
+    kernel_ms = sum(b.elapsed_time(a) for b, a in zip(before, after)) / ksteps
     elapsed_max = max_over_ranks(elapsed_ms, dist)
     value = whole_job_rate(args.steps * w.pixels, elapsed_ms / 1e3, world, dist) / 1e9
 

@@ -36,6 +36,10 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_kernel(const __grid_const
   Scratch* s = p.scratch;
   const int tid = threadIdx.x;
   const int box_bytes = awb_box_bytes(p.raw_format);
+  // The tile pass that follows may launch now: it waits (griddepcontrol.wait)
+  // for this grid's completion before it does anything, but its CTAs become
+  // resident on the SMs this pass leaves while the last tiles are summed.
+  griddep_launch_dependents();
   if constexpr (kWhitePatch) {
     for (int i = tid; i < 3 * kAwbBins; i += kThreads) hist[i] = 0U;
   }

@@ -307,7 +307,21 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
     if (e != cudaSuccess) return e;
   }
   *step = "tile kernel launch";
-  const cudaError_t e = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, need, stream);
+  // After the statistics pass, as its programmatic dependent: the tile pass
+  // becomes resident on the SMs the statistics pass leaves and waits in the
+  // kernel (griddepcontrol.wait) for its completion before anything else. An
+  // event recorded in between (before_main) keeps the two kernels apart.
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = need;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = d.auto_wb ? 1 : 0;
+  const cudaError_t e = cudaLaunchKernelExC(&cfg, k, args);
   if (e != cudaSuccess || after_main == nullptr) return e;
   return cudaEventRecord(after_main, stream);
 }

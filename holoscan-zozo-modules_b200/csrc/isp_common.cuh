@@ -125,6 +125,16 @@ __host__ __device__ constexpr int box_row_bytes(int fmt) {
   return fmt == kRawU8 ? 96 : fmt == kRawU16 ? 160 : fmt == kRawRaw10 ? 112 : 128;
 }
 
+// ---- Programmatic dependent launch ------------------------------------------
+
+// Lets the grid launched after this one (as a programmatic dependent) start
+// before this grid finishes.
+__device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Waits until the grid this one depends on has completed and its memory
+// writes are visible; returns at once when there is no such dependency.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ---- TMA and mbarrier -----------------------------------------------------
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

@@ -285,6 +285,12 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
   __shared__ bool last;
   static_cast<void>(lut_in_smem);
 
+  // Launched as a programmatic dependent of the statistics pass, this kernel
+  // becomes resident on the SMs that pass leaves while it finishes; the wait
+  // returns once the pass has completed and its writes (the gains that
+  // setup_frame reads) are visible. Without a programmatic launch it returns
+  // at once.
+  griddep_wait();
   const FrameSetup f = setup_frame<kLutSmem>(p, m);
   if (threadIdx.x == 0 && use_tma) mbar_init(&bar);
   __syncthreads();
