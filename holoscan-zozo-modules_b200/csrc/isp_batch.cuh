@@ -52,6 +52,9 @@ __global__ void __launch_bounds__(kThreads, 2) isp_batch_kernel(const BatchFrame
   __shared__ int minmax[2];
   __shared__ bool last;
   __shared__ __align__(16) FrameDesc fd;
+  // A programmatic dependent of the statistics batch: resident early, it
+  // waits here for that batch's completion (and the gains it wrote).
+  griddep_wait();
   const int2 r = ranges[blockIdx.x];
   if (r.x >= r.y) return;
   const int tid = threadIdx.x;
@@ -160,6 +163,7 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_batch_kernel(const BatchF
   __shared__ int first;
   __shared__ bool last;
   __shared__ __align__(16) FrameDesc fd;
+  griddep_launch_dependents();  // the tile batch may become resident as this one finishes
   const int2 r = ranges[blockIdx.x];
   if (r.x >= r.y) return;
   const int tid = threadIdx.x;

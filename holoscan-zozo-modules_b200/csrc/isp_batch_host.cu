@@ -205,8 +205,19 @@ cudaError_t enqueue(isp_b200_batch* b, const Slot& slot, const Shape& s, cudaStr
     if (e != cudaSuccess) return e;
   }
   void* args[] = {&b->d_frames, &nframes, &b->d_ranges};
-  return cudaLaunchKernel(batch_kernel(s.lut_smem), dim3(s.main_ctas), dim3(kernel_threads()), args,
-                          batch_kernel_smem(s.lut_smem), stream);
+  // After the statistics batch, as its programmatic dependent (the tile
+  // batch waits for it in the kernel).
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(s.main_ctas);
+  cfg.blockDim = dim3(kernel_threads());
+  cfg.dynamicSmemBytes = batch_kernel_smem(s.lut_smem);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = s.awb_ctas > 0 ? 1 : 0;
+  return cudaLaunchKernelExC(&cfg, batch_kernel(s.lut_smem), args);
 }
 
 // Builds the graph of a shape: the descriptor staging, then the passes.
@@ -244,7 +255,14 @@ cudaError_t make_graph(isp_b200_batch* b, const Slot& slot, const Shape& s) {
   kp.kernelParams = args;
   cudaGraphNode_t main = nullptr;
   if (awb != nullptr) {
-    e = cudaGraphAddKernelNode(&main, b->graph, &awb, 1, &kp);
+    // A programmatic edge from the statistics node, as the direct launch's
+    // attribute: the tile node waits for it in the kernel.
+    e = cudaGraphAddKernelNode(&main, b->graph, nullptr, 0, &kp);
+    if (e != cudaSuccess) return e;
+    cudaGraphEdgeData edge{};
+    edge.from_port = cudaGraphKernelNodePortProgrammatic;
+    edge.type = cudaGraphDependencyTypeProgrammatic;
+    e = cudaGraphAddDependencies_v2(b->graph, &awb, &main, &edge, 1);
   } else {
     e = cudaGraphAddKernelNode(&main, b->graph, &b->stage, 1, &kp);
   }
