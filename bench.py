@@ -22,6 +22,11 @@ from its sources into oracle/_ref) on the host cores, a bounded sample.
 
 --impl reference times that CPU backend alone on the same workload and prints
 the same line with "impl": "reference".
+
+--workload convert measures the colour converter (the step after the ISP):
+a 3840x2160 RGB8 frame into NV12 as the headline line, plus every case of
+the reference converter's benchmark beside the reference's own CUDA kernel
+(built from its sources into oracle/_ref) in a "cases" table.
 """
 from __future__ import annotations
 
