@@ -272,11 +272,11 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
     if (e != cudaSuccess) return e;
     alignas(64) CUtensorMap map;
     int use_tma = encode_raw_map(d, awb_box_row_bytes(d.raw_format), 64, &map) ? 1 : 0;
-    int tiles_x = 0;
-    int tiles = awb_kernel_tiles(d.width, d.height, &tiles_x);
-    const int blocks = std::max(1, std::min(tiles, shapes.sm_count * bpsm));
+    int strips = 0, tiles_y = 0, band_tiles = 0;
+    const int blocks = awb_kernel_bands(d.width, d.height, shapes.sm_count * std::max(bpsm, 1), &strips, &tiles_y,
+                                        &band_tiles);
     FrameDesc desc = d;
-    void* args[] = {&map, &desc, &tiles_x, &tiles, &use_tma};
+    void* args[] = {&map, &desc, &strips, &tiles_y, &band_tiles, &use_tma};
     *step = "white balance kernel launch";
     const cudaError_t e2 = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, smem, stream);
     if (e2 != cudaSuccess) return e2;

@@ -1,5 +1,7 @@
 // isp_kernels.cu - host-side dispatch and launch geometry of the B200 ISP's
 // kernels (isp_main_*.cu, isp_awb.cu).
+#include <algorithm>
+
 #include "isp_common.cuh"
 
 namespace isp_b200 {
@@ -36,10 +38,24 @@ int main_kernel_tiles(int width, int height, int* tiles_x) {
 int kernel_threads() { return kThreads; }
 
 size_t awb_kernel_smem() {
-  // two boxes of 64 x 128, lens shading table, column and row maps, white-patch
-  // histogram, the frame's lens shading grid.
-  return 2U * 64U * 128U + kLscTableRows * 2U * kSW * 4U + 6U * 64U * 4U + 3U * kAwbBins * 4U + kGridSmemGains * 4U +
-         128U;
+  // two boxes of 64 x 128, lens shading table, column maps (64) and row maps
+  // (a band's rows), white-patch histogram, the frame's lens shading grid.
+  return 2U * 64U * 128U + kLscTableRows * 2U * kSW * 4U + 3U * 64U * 4U + 3U * kAwbBandRows * 4U +
+         3U * kAwbBins * 4U + kGridSmemGains * 4U + 128U;
+}
+
+int awb_kernel_bands(int width, int height, int ctas, int* strips, int* tiles_y, int* band_tiles) {
+  // Strips of 64 columns over the complete quads, cut into bands of whole
+  // 64-row tiles: as many bands as let every strip's bands fill `ctas`, each
+  // band at most kAwbBandRows rows, no band empty.
+  const int qw = (width / 2) * 2;
+  const int qh = (height / 2) * 2;
+  *strips = std::max(1, (qw + 63) / 64);
+  *tiles_y = std::max(1, (qh + 63) / 64);
+  int bands = std::max(1, std::min(*tiles_y, ctas / *strips));
+  *band_tiles = std::min((*tiles_y + bands - 1) / bands, kAwbBandRows / 64);
+  bands = (*tiles_y + *band_tiles - 1) / *band_tiles;
+  return *strips * bands;
 }
 
 int awb_box_row_bytes(int raw_format) {

@@ -21,11 +21,16 @@ int main_kernel_tiles(int width, int height, int* tiles_x);
 int kernel_threads();
 
 // The white balance statistics kernel; arguments (const CUtensorMap raw_map,
-// FrameDesc, int tiles_x, int tiles, int use_tma); box awb_box_row_bytes() by 64 rows.
+// FrameDesc, int strips, int tiles_y, int band_tiles, int use_tma), one CTA
+// per band of a strip (awb_kernel_bands); box awb_box_row_bytes() by 64 rows.
 const void* awb_kernel(bool white_patch, int pattern);
 size_t awb_kernel_smem();
 int awb_box_row_bytes(int raw_format);
+// Tiles of 64 x 64 samples over the complete quads (the batch statistics pass).
 int awb_kernel_tiles(int width, int height, int* tiles_x);
+// The single-frame statistics pass's strips and bands for about `ctas` CTAs;
+// returns the CTA count (strips x bands).
+int awb_kernel_bands(int width, int height, int ctas, int* strips, int* tiles_y, int* band_tiles);
 
 // Tone tables up to this many entries may be copied into shared memory.
 constexpr int kLutSmemEntries = 4097;

@@ -111,11 +111,11 @@ cudaError_t launch_noalloc(const FrameDesc& d, const isp_params_c& p, int sm_cou
     if (e != cudaSuccess) return e;
     alignas(64) CUtensorMap map;
     int use_tma = encode_raw_map(d, awb_box_row_bytes(d.raw_format), 64, &map) ? 1 : 0;
-    int tiles_x = 0;
-    int tiles = awb_kernel_tiles(d.width, d.height, &tiles_x);
-    const int blocks = std::max(1, std::min(tiles, sm_count * std::max(bpsm, 1)));
+    int strips = 0, tiles_y = 0, band_tiles = 0;
+    const int blocks = awb_kernel_bands(d.width, d.height, sm_count * std::max(bpsm, 1), &strips, &tiles_y,
+                                        &band_tiles);
     FrameDesc desc = d;
-    void* args[] = {&map, &desc, &tiles_x, &tiles, &use_tma};
+    void* args[] = {&map, &desc, &strips, &tiles_y, &band_tiles, &use_tma};
     e = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, smem, stream);
     if (e != cudaSuccess) return e;
   }

@@ -15,6 +15,7 @@ enum : int { kWbManual = 0, kWbGrayWorld = 1, kWbWhitePatch = 2 };
 
 constexpr float kFixedOne = 1048576.0F;  // statistics' fixed point: 2^-20 units
 constexpr int kAwbBins = 1024;           // white-patch histogram bins
+constexpr int kAwbBandRows = 1024;       // most rows of one statistics band (16 tiles of 64)
 constexpr int kHistBins = 256;
 constexpr int kHistChannels = 4;
 constexpr int kStatsSize = 12;
