@@ -285,6 +285,20 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
   __shared__ bool last;
   static_cast<void>(lut_in_smem);
 
+  const int fmt = p.raw_format;
+  const auto issue = [&](int t) {
+    const int ty = t / tiles_x;
+    const int x0 = (t - ty * tiles_x) * kTW;
+    tma_load_2d(&map, m.box, &bar, box_x(fmt, x0), ty * kTH - G::kHalo, static_cast<unsigned int>(G::kSH * box_bytes));
+  };
+  // The first tile's box reads only the input frame: it is requested before
+  // the wait below (the barrier initialised and made visible to the copy
+  // engine first; the other threads meet it after the block barrier).
+  if (use_tma && threadIdx.x == 0) {
+    mbar_init(&bar);
+    fence_async_shared();
+    if (static_cast<int>(blockIdx.x) < tiles) issue(blockIdx.x);
+  }
   // Launched as a programmatic dependent of the statistics pass, this kernel
   // becomes resident on the SMs that pass leaves while it finishes; the wait
   // returns once the pass has completed and its writes (the gains that
@@ -292,18 +306,10 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
   // at once.
   griddep_wait();
   const FrameSetup f = setup_frame<kLutSmem>(p, m);
-  if (threadIdx.x == 0 && use_tma) mbar_init(&bar);
   __syncthreads();
 
-  const int fmt = p.raw_format;
   u64 acc[4] = {0, 0, 0, 0};  // linear R, G, B in 2^-20 units; saturated samples
   uint32_t phase = 0;
-  const auto issue = [&](int t) {
-    const int ty = t / tiles_x;
-    const int x0 = (t - ty * tiles_x) * kTW;
-    tma_load_2d(&map, m.box, &bar, box_x(fmt, x0), ty * kTH - G::kHalo, static_cast<unsigned int>(G::kSH * box_bytes));
-  };
-  if (use_tma && threadIdx.x == 0 && static_cast<int>(blockIdx.x) < tiles) issue(blockIdx.x);
   unsigned int done = 0;
   for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const int ty = tile / tiles_x;
