@@ -907,6 +907,34 @@ def cc_time(torch, launch, nset: int, calls: int, rounds: int, warmup: int, stre
     return best
 
 
+def cc_graph_time(torch, launch, nset: int, calls: int) -> float:
+    """Mean ms per call of `calls` calls (rotating over `nset` buffer sets)
+    captured in one CUDA graph; best of three replays after a warm one."""
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        for j in range(3):
+            launch(j % nset, side.cuda_stream)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side):
+        for j in range(calls):
+            launch(j % nset, side.cuda_stream)
+    graph.replay()
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(3):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(side)
+        with torch.cuda.stream(side):
+            graph.replay()
+        b.record(side)
+        b.synchronize()
+        ms = a.elapsed_time(b) / calls
+        best = ms if best is None else min(best, ms)
+    del graph
+    return best
+
+
 def run_convert(args):
     """The colour converter: the headline case (a 3840x2160 RGB8 frame, the
     ISP's output, into NV12) timed as the contract asks, then every case of
@@ -1073,11 +1101,21 @@ def run_convert(args):
                     if have_ref:
                         ref = cc_time(torch, lambda j: occ.ref_cuda_convert(vv[j][0], vv[j][1], cp, sptr), k, calls, 3,
                                       50, stream)
+                # The same calls captured once in a CUDA graph and replayed: the
+                # kernels without the host launch path (both implementations).
+                ours_g = cc_graph_time(torch, lambda j, sp: conv.convert(vv[j][0], vv[j][1], cp, sp), k, calls)
+                ref_g = None
+                if have_ref:
+                    ref_g = cc_graph_time(torch, lambda j, sp: occ.ref_cuda_convert(vv[j][0], vv[j][1], cp, sp), k,
+                                          calls)
                 cases.append({"input": f"{cc.format_name(src)} {w}x{h}", "output": f"{cc.format_name(dst)} {dw}x{dh}",
                               "operation": label, "ms": round(ours, 5),
                               "reference_kernel_ms": None if ref is None else round(ref, 5),
                               "speedup": None if ref is None else round(ref / ours, 3),
-                              "gbs": round(per / (ours / 1e3) / 1e9, 1)})
+                              "gbs": round(per / (ours / 1e3) / 1e9, 1),
+                              "graph_ms": round(ours_g, 5),
+                              "reference_kernel_graph_ms": None if ref_g is None else round(ref_g, 5),
+                              "graph_speedup": None if ref_g is None else round(ref_g / ours_g, 3)})
                 del ins, outs, vv
 
     cpu = None
