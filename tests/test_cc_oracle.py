@@ -239,3 +239,37 @@ def test_oracle_matches_golden_fixtures():
         img = occ.noise(int(src), int(sw), int(sh), int(seed))
         got = occ.convert(img, int(src), int(sw), int(sh), int(dst), int(dw), int(dh), p)
         assert np.array_equal(got, data[f"out{i}"]), (i, NAMES[src], NAMES[dst])
+
+
+@need_ref
+def test_validation_matches_reference_fuzz():
+    """Random views and settings: the converter's checks accept exactly what
+    the reference's validate_conversion accepts and refuse the rest with its
+    message (conversion.cpp:170-192, :403-408)."""
+    rng = np.random.default_rng(11)
+    buf = np.zeros(1 << 16, np.uint8)
+    for _ in range(2000):
+        views = []
+        for _side in range(2):
+            fmt = int(rng.integers(0, 12))
+            w, h = int(rng.integers(-2, 40)), int(rng.integers(-2, 30))
+            v = occ.host_view(buf, fmt, max(w, 1), max(h, 1), location=cc.DEVICE)
+            v.width, v.height = w, h
+            for k in range(3):
+                if rng.random() < 0.05:
+                    v.planes[k].data = None
+                if rng.random() < 0.1:
+                    v.planes[k].pitch = max(0, int(v.planes[k].pitch) - int(rng.integers(1, 4)))
+            views.append(v)
+        crop = None
+        if rng.random() < 0.4:
+            crop = tuple(int(x) for x in rng.integers(-3, 45, 4))
+        p = cc.params(int(rng.integers(0, 3)), int(rng.integers(0, 2)), int(rng.integers(0, 3)), crop,
+                      bool(rng.random() < 0.5))
+        want = occ.ref_validate(views[0], views[1], p)
+        try:
+            cc.validate_conversion(views[0], views[1], p)
+            got = None
+        except ValueError as e:
+            got = str(e)
+        assert got == want, (got, want)
