@@ -61,7 +61,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c3", "c4", "convert"], default="c1")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c3", "c4", "convert", "view"], default="c1")
     ap.add_argument("--seconds", type=float, default=60.0, help="c4: the nominal-rate serving run")
     ap.add_argument("--aux-seconds", type=float, default=15.0, help="c4: the other serving runs")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
@@ -1238,14 +1238,180 @@ def run_convert_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---- The demo's side-by-side view -------------------------------------------
+
+VIEW_METRIC = "side-by-side view Gpix/s (bit-exact vs the C restatement)"
+
+
+def run_view(args):
+    """isp_b200_view_compose on a 3840x2160 RAW10 frame and its RGB8 image
+    into the 7680x2160 RGB8 view: device-resident throughput over rotating
+    buffer sets larger than L2, the kernel's roofline, and the C restatement
+    (oracle_view_compose) on the host cores as the CPU baseline (the demo's
+    own kernel needs the Holoscan SDK)."""
+    import torch
+
+    import isp_b200
+    import oracle
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    w, h, black = 3840, 2160, 64.0
+    rng = np.random.default_rng(5 + rank)
+    pitch = abi.raw_row_bytes(abi.RAW10, w)
+    raw = abi.RawFrame(rng.integers(0, 256, pitch * h, dtype=np.uint8), w, h, pitch, abi.RAW10, 10, abi.GRBG)
+    rgb = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+    per = pitch * h + 3 * w * h + 6 * w * h
+    nset = max(2, math.ceil(2 * L2_BYTES / per))
+    d_raw = [torch.from_numpy(raw.data).cuda() for _ in range(nset)]
+    d_rgb = [torch.from_numpy(rgb.reshape(-1)).cuda() for _ in range(nset)]
+    d_out = [torch.empty(6 * w * h, dtype=torch.uint8, device="cuda") for _ in range(nset)]
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+
+    def step(i):
+        k = i % nset
+        isp_b200.view_compose(raw.view(d_raw[k].data_ptr()), black, d_rgb[k].data_ptr(), 3 * w, d_out[k].data_ptr(),
+                              6 * w, sptr)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+        torch.cuda.synchronize()
+        clocks = Clocks(local)
+        clocks.start()
+        time.sleep(0.3)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for i in range(args.steps):
+            step(i)
+        b.record(stream)
+        b.synchronize()
+        clock_info = clocks.stop()
+    ms = a.elapsed_time(b) / args.steps
+    value = whole_job_rate(args.steps * w * h, ms * args.steps / 1e3, world, None) / 1e9
+    got = d_out[0].cpu().numpy().reshape(h, 2 * w, 3)
+    verified = bool(np.array_equal(got, oracle.view_compose(raw, black, rgb)))
+
+    # End to end: the raw frame and the RGB8 image from pinned host memory, the view back, every step.
+    h_raw = torch.from_numpy(raw.data).pin_memory()
+    h_rgb = torch.from_numpy(rgb.reshape(-1)).pin_memory()
+    h_out = torch.empty(6 * w * h, dtype=torch.uint8).pin_memory()
+    e2e_steps = max(3, min(args.steps, 100))
+    with torch.cuda.stream(stream):
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ea.record(stream)
+        for _ in range(e2e_steps):
+            d_raw[0].copy_(h_raw, non_blocking=True)
+            d_rgb[0].copy_(h_rgb, non_blocking=True)
+            step(0)
+            h_out.copy_(d_out[0], non_blocking=True)
+        eb.record(stream)
+        eb.synchronize()
+    e2e_value = e2e_steps * w * h / (ea.elapsed_time(eb) / 1e3) / 1e9
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        threads = cpu_threads()
+        rows = 64
+        band = abi.RawFrame(raw.data[: rows * pitch], w, rows, pitch, abi.RAW10, 10, abi.GRBG)
+        counts = [0] * threads
+        stop = time.perf_counter() + args.cpu_seconds
+
+        def work(i):
+            while time.perf_counter() < stop or counts[i] == 0:
+                oracle.view_compose(band, black, rgb[:rows])
+                counts[i] += 1
+
+        t0 = time.perf_counter()
+        ts = [threading.Thread(target=work, args=(i,)) for i in range(threads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        secs = time.perf_counter() - t0
+        cpu = {"value": sum(counts) * w * rows / secs / 1e9, "unit": "Gpix/s", "cores": threads, "kind": "port",
+               "sample": f"{sum(counts)} bands of {w}x{rows} over {secs:.1f} s on {threads} threads"}
+
+    peak, peak_kind = measured_peak()
+    achieved = per / (ms / 1e3) / 1e9
+    line = {
+        "metric": VIEW_METRIC, "value": value, "unit": "Gpix/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (random RAW10 frame and RGB8 image)",
+        "config": {"workload": "view_3840x2160_raw10", "view": "7680x2160 RGB8", "black_level": black,
+                   "compulsory_bytes_per_frame": per,
+                   "l2": f"{nset} rotating buffer sets, {nset * per / 1e6:.0f} MB > 126 MB L2",
+                   "verified_bit_exact": verified},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "isp_view_kernel", "kernel_ms": ms, "peak_kind": peak_kind},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "Gpix/s", "h2d_bytes_per_step": pitch * h + 3 * w * h,
+                "d2h_bytes_per_step": 6 * w * h, "steps": e2e_steps,
+                "api": "isp_b200_view_compose between pinned-host copies, one stream"},
+        "gpu_launches": args.steps,
+        "clocks": clock_info,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_view_reference(args):
+    """--impl reference --workload view: the demo's view kernel needs the
+    Holoscan SDK, so the reference arm times its C restatement
+    (oracle_view_compose) on the host cores, bands of the same frame."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+
+    w, rows, black = 3840, 64, 64.0
+    rng = np.random.default_rng(5)
+    pitch = abi.raw_row_bytes(abi.RAW10, w)
+    band = abi.RawFrame(rng.integers(0, 256, pitch * rows, dtype=np.uint8), w, rows, pitch, abi.RAW10, 10, abi.GRBG)
+    rgb = rng.integers(0, 256, (rows, w, 3), dtype=np.uint8)
+    threads = cpu_threads()
+
+    def step():
+        t0 = time.perf_counter()
+        ts = [threading.Thread(target=oracle.view_compose, args=(band, black, rgb)) for _ in range(threads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        return time.perf_counter() - t0
+
+    times = []
+    for i in range(min(args.warmup, 3) + min(args.steps, 50)):
+        t = step()
+        if i >= min(args.warmup, 3):
+            times.append(t)
+    total = sum(times)
+    value = threads * w * rows * len(times) / total / 1e9
+    line = {
+        "metric": VIEW_METRIC, "value": value, "unit": "Gpix/s", "n_gpus": args.gpus, "steps": len(times),
+        "warmup": min(args.warmup, 3), "ms_per_step": total / len(times) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (random RAW10 frame and RGB8 image)",
+        "config": {"workload": "view_3840x2160_raw10"}, "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "Gpix/s", "cores": threads, "kind": "port",
+                         "sample": f"{threads} threads x one {w}x{rows} band per step"},
+        "e2e": {"value": value, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
-    if args.impl == "reference" and args.workload == "convert":
+    if args.impl == "reference" and args.workload == "view":
+        run_view_reference(args)
+    elif args.impl == "reference" and args.workload == "convert":
         run_convert_reference(args)
     elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "convert":
         run_convert(args)
+    elif args.workload == "view":
+        run_view(args)
     elif args.workload == "c3":
         run_batch(args)
     elif args.workload == "c4":

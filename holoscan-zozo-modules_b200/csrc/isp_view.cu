@@ -1,8 +1,8 @@
 // isp_view.cu - the demo's side-by-side view of raw and processed frames
 // (applications/isp/src/view_op.cu:35-75), as a headless device image: the
 // raw mosaic as square-rooted gray on the left, the ISP's RGB8 image on the
-// right. One thread converts four pixels of a row (one RAW10 group, two RAW12
-// groups) and copies the four RGB pixels beside them.
+// right. One thread converts a run of sixteen pixels of a row and copies
+// the sixteen RGB pixels beside them.
 #include <cuda_runtime.h>
 
 #include <string>
@@ -47,31 +47,55 @@ __device__ __forceinline__ uint32_t view_gray(int s, float black, float scale) {
   return __float2uint_rz(__fadd_rn(__fmul_rn(__fsqrt_rn(v), 255.0F), 0.5F));
 }
 
+// One thread per run of 16 pixels of a row (x0 = 16 g): their 16 gray codes
+// and the 16 RGB pixels beside them. Where the rows allow it (16-byte aligned
+// RGB and view rows, a whole run inside the frame) the 48-byte runs move as
+// three 16-byte words each and the raw samples come as 32-bit words; else
+// byte by byte.
 __global__ void __launch_bounds__(256) isp_view_kernel(const __grid_constant__ ViewArgs a) {
-  const int x0 = 4 * static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+  constexpr int kRun = 16;
+  const int x0 = kRun * static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
   const int y = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
   if (x0 >= a.width || y >= a.height) return;
-  const int n = a.width - x0 < 4 ? a.width - x0 : 4;
+  const int n = a.width - x0 < kRun ? a.width - x0 : kRun;
   const uint8_t* raw = a.raw + static_cast<size_t>(y) * a.raw_pitch;
   const uint8_t* rgb = a.rgb + static_cast<size_t>(y) * a.rgb_pitch + 3 * static_cast<size_t>(x0);
   uint8_t* left = a.out + static_cast<size_t>(y) * a.out_pitch + 3 * static_cast<size_t>(x0);
   uint8_t* right = left + 3 * static_cast<size_t>(a.width);
-  uint8_t g[4], c[12];
+  const bool vec = n == kRun && ((reinterpret_cast<uintptr_t>(rgb) | reinterpret_cast<uintptr_t>(left) |
+                                  reinterpret_cast<uintptr_t>(right)) & 15U) == 0U;
+  if (vec) {
+    // The RGB run: three 16-byte words, loaded before the arithmetic.
+    const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(rgb));
+    const uint4 c1 = __ldg(reinterpret_cast<const uint4*>(rgb) + 1);
+    const uint4 c2 = __ldg(reinterpret_cast<const uint4*>(rgb) + 2);
+    uint32_t g[kRun];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    if (i < n) {
-      g[i] = static_cast<uint8_t>(view_gray(view_sample(raw, a.format, x0 + i), a.black, a.scale));
+    for (int i = 0; i < kRun; ++i) g[i] = view_gray(view_sample(raw, a.format, x0 + i), a.black, a.scale);
+    // Gray pixels: bytes g, g, g per pixel, 48 bytes as 12 words.
+    uint32_t w[12];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) c[3 * i + k] = __ldg(rgb + 3 * i + k);
+    for (int k = 0; k < 12; ++k) {
+      uint32_t v = 0U;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) v |= g[(4 * k + b) / 3] << (8 * b);
+      w[k] = v;
     }
+    uint4* l = reinterpret_cast<uint4*>(left);
+    l[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    l[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    l[2] = make_uint4(w[8], w[9], w[10], w[11]);
+    uint4* r = reinterpret_cast<uint4*>(right);
+    r[0] = c0;
+    r[1] = c1;
+    r[2] = c2;
+    return;
   }
+  for (int i = 0; i < n; ++i) {
+    const uint8_t g = static_cast<uint8_t>(view_gray(view_sample(raw, a.format, x0 + i), a.black, a.scale));
+    left[3 * i] = left[3 * i + 1] = left[3 * i + 2] = g;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    if (i < n) {
-      left[3 * i] = left[3 * i + 1] = left[3 * i + 2] = g[i];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) right[3 * i + k] = c[3 * i + k];
-    }
+    for (int k = 0; k < 3; ++k) right[3 * i + k] = __ldg(rgb + 3 * i + k);
   }
 }
 
@@ -101,7 +125,7 @@ extern "C" ISP_B200_API int isp_b200_view_compose(const isp_raw_view_c* raw, flo
              1.0F / (white - black_level), static_cast<const uint8_t*>(rgb8), rgb8_pitch,
              static_cast<uint8_t*>(view), view_pitch};
   const dim3 block(32, 8);
-  const dim3 grid(static_cast<unsigned>((raw->width + 127) / 128), static_cast<unsigned>((raw->height + 7) / 8));
+  const dim3 grid(static_cast<unsigned>((raw->width + 511) / 512), static_cast<unsigned>((raw->height + 7) / 8));
   isp_view_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(a);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail_cuda(e, "view kernel");
