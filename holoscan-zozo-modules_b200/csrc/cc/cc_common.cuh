@@ -242,25 +242,46 @@ __device__ __forceinline__ bool fetch4(const Image& img, int sx, int sy, uint32_
   return true;
 }
 
+// Two bytes (byte ka of wa, byte kb of wb) as the floats of two lanes: the
+// 2^23-biased bits of each, less 2^23 two lanes at a time (an exact result).
+__device__ __forceinline__ float2 bytes2(uint32_t wa, int ka, uint32_t wb, int kb) {
+  const float2 biased = make_float2(__uint_as_float(__byte_perm(wa, kTwo23Bits, 0x7650U | static_cast<uint32_t>(ka))),
+                                    __uint_as_float(__byte_perm(wb, kTwo23Bits, 0x7650U | static_cast<uint32_t>(kb))));
+  float2 r;
+  asm("{ .reg .b64 a, b, d; mov.b64 a, {%2, %3}; mov.b64 b, {%4, %5}; sub.rn.f32x2 d, a, b; mov.b64 {%0, %1}, d; }"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(biased.x), "f"(biased.y), "f"(kTwo23), "f"(kTwo23));
+  return r;
+}
+
 template <int kF>
 __device__ __forceinline__ void decode4(const uint32_t (&w)[kRawWords], Px (&s)[4]) {
   if constexpr (kF == CC_RGB8 || kF == CC_BGR8) {
+    // Pixels (0, 1) and (2, 3) as lane pairs, channel by channel.
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const float a = byte_of(w[(3 * i) >> 2], (3 * i) & 3);
-      const float b = byte_of(w[(3 * i + 1) >> 2], (3 * i + 1) & 3);
-      const float c = byte_of(w[(3 * i + 2) >> 2], (3 * i + 2) & 3);
-      s[i] = kF == CC_RGB8 ? Px{a, b, c, 255.0F} : Px{c, b, a, 255.0F};
+    for (int i = 0; i < 4; i += 2) {
+      float2 c[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        c[j] = bytes2(w[(3 * i + j) >> 2], (3 * i + j) & 3, w[(3 * (i + 1) + j) >> 2], (3 * (i + 1) + j) & 3);
+      }
+      s[i] = kF == CC_RGB8 ? Px{c[0].x, c[1].x, c[2].x, 255.0F} : Px{c[2].x, c[1].x, c[0].x, 255.0F};
+      s[i + 1] = kF == CC_RGB8 ? Px{c[0].y, c[1].y, c[2].y, 255.0F} : Px{c[2].y, c[1].y, c[0].y, 255.0F};
     }
   } else if constexpr (kF == CC_RGBA8 || kF == CC_BGRA8) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const float a = byte_of(w[i], 0), b = byte_of(w[i], 1), c = byte_of(w[i], 2), al = byte_of(w[i], 3);
-      s[i] = kF == CC_RGBA8 ? Px{a, b, c, al} : Px{c, b, a, al};
+    for (int i = 0; i < 4; i += 2) {
+      const float2 a = bytes2(w[i], 0, w[i + 1], 0), b = bytes2(w[i], 1, w[i + 1], 1);
+      const float2 c = bytes2(w[i], 2, w[i + 1], 2), al = bytes2(w[i], 3, w[i + 1], 3);
+      s[i] = kF == CC_RGBA8 ? Px{a.x, b.x, c.x, al.x} : Px{c.x, b.x, a.x, al.x};
+      s[i + 1] = kF == CC_RGBA8 ? Px{a.y, b.y, c.y, al.y} : Px{c.y, b.y, a.y, al.y};
     }
   } else if constexpr (kF == CC_MONO8) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) s[i] = Px{byte_of(w[0], i), 0.0F, 0.0F, 255.0F};
+    const float2 a = bytes2(w[0], 0, w[0], 1), b = bytes2(w[0], 2, w[0], 3);
+    s[0] = Px{a.x, 0.0F, 0.0F, 255.0F};
+    s[1] = Px{a.y, 0.0F, 0.0F, 255.0F};
+    s[2] = Px{b.x, 0.0F, 0.0F, 255.0F};
+    s[3] = Px{b.y, 0.0F, 0.0F, 255.0F};
   } else if constexpr (kF == CC_MONO16) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) s[i] = Px{div257((w[i >> 1] >> (16 * (i & 1))) & 0xFFFFU), 0.0F, 0.0F, 255.0F};
@@ -273,18 +294,22 @@ __device__ __forceinline__ void decode4(const uint32_t (&w)[kRawWords], Px (&s)[
       s[i] = Px{c[0], c[1], c[2], 255.0F};
     }
   } else if constexpr (kF == CC_NV12 || kF == CC_NV16 || kF == CC_I420) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      s[i] = Px{byte_of(w[0], i), byte_of(w[1], 2 * (i >> 1)), byte_of(w[1], 2 * (i >> 1) + 1), 255.0F};
-    }
+    // Luma of pixels (0, 1) and (2, 3); the two chroma pairs (Cb, Cr) of the run.
+    const float2 y01 = bytes2(w[0], 0, w[0], 1), y23 = bytes2(w[0], 2, w[0], 3);
+    const float2 cb = bytes2(w[1], 0, w[1], 2), cr = bytes2(w[1], 1, w[1], 3);
+    s[0] = Px{y01.x, cb.x, cr.x, 255.0F};
+    s[1] = Px{y01.y, cb.x, cr.x, 255.0F};
+    s[2] = Px{y23.x, cb.y, cr.y, 255.0F};
+    s[3] = Px{y23.y, cb.y, cr.y, 255.0F};
   } else {
     constexpr int kY = kF == CC_YUYV ? 0 : 1;  // byte of the first luma in a pair
     constexpr int kU = kF == CC_YUYV ? 1 : 0;  // byte of Cb; Cr two later
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const uint32_t q = w[i >> 1];
-      s[i] = Px{byte_of(q, kY + 2 * (i & 1)), byte_of(q, kU), byte_of(q, kU + 2), 255.0F};
-    }
+    const float2 y01 = bytes2(w[0], kY, w[0], kY + 2), y23 = bytes2(w[1], kY, w[1], kY + 2);
+    const float2 cb = bytes2(w[0], kU, w[1], kU), cr = bytes2(w[0], kU + 2, w[1], kU + 2);
+    s[0] = Px{y01.x, cb.x, cr.x, 255.0F};
+    s[1] = Px{y01.y, cb.x, cr.x, 255.0F};
+    s[2] = Px{y23.x, cb.y, cr.y, 255.0F};
+    s[3] = Px{y23.y, cb.y, cr.y, 255.0F};
   }
 }
 

@@ -121,6 +121,20 @@ __device__ __forceinline__ void affine_pair(const Plan& p, Px& a, Px& b) {
   }
 }
 
+// code8_bits of two values: the + 0.5 and the add of 2^23 rounded toward
+// zero (equal to rounding down, the value being clamped to [0, 255]) two
+// lanes at a time, the clamps per lane. Neither add consumes a product, so
+// nothing can be fused into it.
+__device__ __forceinline__ uint2 code8_bits2(float a, float b) {
+  using isp_b200::add2;
+  using isp_b200::add2_rz;
+  using isp_b200::bc2;
+  const float2 h = add2(make_float2(a, b), bc2(0.5F));
+  const float2 c = make_float2(fminf(fmaxf(h.x, 0.0F), 255.0F), fminf(fmaxf(h.y, 0.0F), 255.0F));
+  const float2 r = add2_rz(c, bc2(kTwo23));
+  return make_uint2(__float_as_uint(r.x), __float_as_uint(r.y));
+}
+
 // One four-pixel row segment of format kDst at (x, y) from whole, aligned
 // groups: every word of it stored, the row start known to be 4-byte aligned.
 // Codes come as their 2^23-biased bits (code8_bits / code16_bits); cb and cr
@@ -130,23 +144,29 @@ __device__ __forceinline__ void store_full4(const Image& img, int x, int y, cons
                                             const uint32_t (&cb)[2], const uint32_t (&cr)[2]) {
   uint8_t* row = img.data[0] + static_cast<size_t>(y) * img.pitch[0];
   if constexpr (kDst == CC_NV12 || kDst == CC_NV16 || kDst == CC_I420 || kDst == CC_MONO8) {
-    *reinterpret_cast<uint32_t*>(row + x) =
-        pack8(code8_bits(v[0].c0), code8_bits(v[1].c0), code8_bits(v[2].c0), code8_bits(v[3].c0));
+    const uint2 a = code8_bits2(v[0].c0, v[1].c0), b = code8_bits2(v[2].c0, v[3].c0);
+    *reinterpret_cast<uint32_t*>(row + x) = pack8(a.x, a.y, b.x, b.y);
   } else if constexpr (kDst == CC_YUYV || kDst == CC_UYVY) {
     uint32_t* q = reinterpret_cast<uint32_t*>(row + 2 * x);
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-      const uint32_t y0 = code8_bits(v[2 * k].c0), y1 = code8_bits(v[2 * k + 1].c0);
-      q[k] = kDst == CC_YUYV ? pack8(y0, cb[k], y1, cr[k]) : pack8(cb[k], y0, cr[k], y1);
+      const uint2 yy = code8_bits2(v[2 * k].c0, v[2 * k + 1].c0);
+      q[k] = kDst == CC_YUYV ? pack8(yy.x, cb[k], yy.y, cr[k]) : pack8(cb[k], yy.x, cr[k], yy.y);
     }
   } else if constexpr (kDst == CC_RGB8 || kDst == CC_BGR8) {
     const bool bgr = kDst == CC_BGR8;
     uint32_t b[12];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      b[3 * i] = code8_bits(bgr ? v[i].c2 : v[i].c0);
-      b[3 * i + 1] = code8_bits(v[i].c1);
-      b[3 * i + 2] = code8_bits(bgr ? v[i].c0 : v[i].c2);
+    for (int i = 0; i < 4; i += 2) {
+      const uint2 r = code8_bits2(bgr ? v[i].c2 : v[i].c0, bgr ? v[i + 1].c2 : v[i + 1].c0);
+      const uint2 g = code8_bits2(v[i].c1, v[i + 1].c1);
+      const uint2 bl = code8_bits2(bgr ? v[i].c0 : v[i].c2, bgr ? v[i + 1].c0 : v[i + 1].c2);
+      b[3 * i] = r.x;
+      b[3 * i + 1] = g.x;
+      b[3 * i + 2] = bl.x;
+      b[3 * i + 3] = r.y;
+      b[3 * i + 4] = g.y;
+      b[3 * i + 5] = bl.y;
     }
     uint32_t* q = reinterpret_cast<uint32_t*>(row + 3 * x);
 #pragma unroll
@@ -155,9 +175,13 @@ __device__ __forceinline__ void store_full4(const Image& img, int x, int y, cons
     const bool bgr = kDst == CC_BGRA8;
     uint32_t* q = reinterpret_cast<uint32_t*>(row + 4 * x);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      q[i] = pack8(code8_bits(bgr ? v[i].c2 : v[i].c0), code8_bits(v[i].c1), code8_bits(bgr ? v[i].c0 : v[i].c2),
-                   code8_bits(v[i].a));
+    for (int i = 0; i < 4; i += 2) {
+      const uint2 r = code8_bits2(bgr ? v[i].c2 : v[i].c0, bgr ? v[i + 1].c2 : v[i + 1].c0);
+      const uint2 g = code8_bits2(v[i].c1, v[i + 1].c1);
+      const uint2 bl = code8_bits2(bgr ? v[i].c0 : v[i].c2, bgr ? v[i + 1].c0 : v[i + 1].c2);
+      const uint2 al = code8_bits2(v[i].a, v[i + 1].a);
+      q[i] = pack8(r.x, g.x, bl.x, al.x);
+      q[i + 1] = pack8(r.y, g.y, bl.y, al.y);
     }
   } else if constexpr (kDst == CC_MONO16) {
     uint32_t* q = reinterpret_cast<uint32_t*>(row + 2 * x);
