@@ -67,6 +67,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cases", action="store_true", help="convert: the headline case only")
+    ap.add_argument("--fresh-frames", type=int, default=0,
+                    help="c2: render this many fresh-seed frames instead of the workload's 200 (small profiling runs)")
     return ap.parse_args()
 
 
@@ -306,6 +308,8 @@ def run_b200(args):
         torch.cuda.synchronize()
 
     w = WORKLOADS[args.workload]()
+    if args.fresh_frames > 0 and w.fresh_frames:
+        w.fresh_frames = args.fresh_frames
     raw = w.raw(1 + rank)
     out_row = w.width * abi.output_channels(w.out_format) * abi.output_channel_bytes(w.out_format)
     nbuf = max(2, math.ceil(2 * L2_BYTES / w.compulsory_bytes()))
