@@ -455,6 +455,46 @@ def run_b200(args):
     e2e_stream_s = time.perf_counter() - t0
     e2e_value = whole_job_rate(stream_steps * w.pixels, e2e_stream_s, world, dist) / 1e9
 
+    # The reference's own CUDA backend for sm_100a on the same device frames,
+    # stream and step, after the timed region (the GPU bar; not this build).
+    ref_gpu = None
+    if rank == 0 and world == 1:
+        import oracle
+
+        if oracle.reference_cuda_available():
+            rp = oracle.ReferenceCudaPipeline(w.params)
+            rsteps = min(args.steps, 400)
+            with torch.cuda.stream(stream):
+                for i in range(10):
+                    rv, ov, st = views[i % len(views)]
+                    rp.process(rv, ov, st, exp, stream.cuda_stream)
+                ra, rb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ra.record(stream)
+                for i in range(rsteps):
+                    rv, ov, st = views[i % len(views)]
+                    rp.process(rv, ov, st, exp, stream.cuda_stream)
+                rb.record(stream)
+                rb.synchronize()
+            rms = ra.elapsed_time(rb) / rsteps
+            # One frame from each, byte for byte (informational).
+            rv, ov, st = views[0]
+            torch.cuda.synchronize()
+            rp.close()
+            pipe.reset()
+            rp2 = oracle.ReferenceCudaPipeline(w.params)
+            rp2.process(rv, ov, st, exp, 0)
+            torch.cuda.synchronize()
+            theirs = outs[0].cpu().numpy().copy()
+            rp2.close()
+            isp_b200.check(L.isp_b200_process(pipe.handle, C.byref(rv), C.byref(ov), C.byref(st), C.byref(exp), None))
+            torch.cuda.synchronize()
+            same = bool(np.array_equal(theirs, outs[0].cpu().numpy()))
+            ref_gpu = {"value": w.pixels / (rms / 1e3) / 1e9, "unit": "Gpix/s", "ms_per_step": rms, "steps": rsteps,
+                       "speedup_of_this_build": (rms / 1e3) / (elapsed_ms / 1e3 / args.steps),
+                       "image_bytes_equal": same,
+                       "library": "oracle/_ref/libisp_ref_cuda.so (the reference's cuda_pipeline.cu, sm_100a, "
+                                  "--fmad=false)"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
@@ -485,6 +525,7 @@ def run_b200(args):
                     "synchronous_api": "isp_b200_process_host (one frame at a time, copies not overlapped)"},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clock_info,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

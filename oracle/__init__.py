@@ -80,6 +80,48 @@ def reference_available() -> bool:
     return os.path.exists(REF_SO)
 
 
+REF_CUDA_SO = os.path.join(_HERE, "_ref", "libisp_ref_cuda.so")
+_ref_cuda = None
+
+
+def reference_cuda_available() -> bool:
+    return os.path.exists(REF_CUDA_SO)
+
+
+class ReferenceCudaPipeline:
+    """The reference's own CUDA backend (IspPipeline(Backend::kCuda), built
+    for sm_100a into oracle/_ref/libisp_ref_cuda.so): device views, frames
+    queued on a stream. The GPU bar of the benchmark, not a checker."""
+
+    def __init__(self, params: abi.IspParams):
+        global _ref_cuda
+        if _ref_cuda is None:
+            lib = C.CDLL(REF_CUDA_SO)
+            P = C.POINTER
+            lib.ref_cuda_pipeline_create.restype = C.c_void_p
+            lib.ref_cuda_pipeline_create.argtypes = [P(abi.ParamsC)]
+            lib.ref_cuda_pipeline_destroy.argtypes = [C.c_void_p]
+            lib.ref_cuda_pipeline_process.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
+                                                      P(abi.ExposureC), C.c_void_p]
+            _ref_cuda = lib
+        self.lib = _ref_cuda
+        self.holder = params.to_c()
+        self.handle = self.lib.ref_cuda_pipeline_create(self.holder.ref())
+        if not self.handle:
+            raise RuntimeError("the reference CUDA pipeline could not be created")
+
+    def process(self, raw: abi.RawViewC, out: abi.RgbViewC, stats: abi.StatsC, exposure: abi.ExposureC,
+                stream: int) -> None:
+        if self.lib.ref_cuda_pipeline_process(self.handle, C.byref(raw), C.byref(out), C.byref(stats),
+                                              C.byref(exposure), C.c_void_p(stream)) != 0:
+            raise RuntimeError("the reference CUDA pipeline failed")
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.ref_cuda_pipeline_destroy(self.handle)
+            self.handle = None
+
+
 def _lib_ref():
     global _ref
     if _ref is None:

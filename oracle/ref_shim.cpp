@@ -19,6 +19,11 @@
 
 #include "cpu_pipeline.hpp"
 #include "holoscan/isp/isp_params.hpp"
+#ifdef ISP_REF_CUDA
+#include <cuda_runtime_api.h>
+
+#include "holoscan/isp/isp_pipeline.hpp"
+#endif
 #include "holoscan/isp/synthetic_raw.hpp"
 #include "isp_b200.h"
 
@@ -275,5 +280,36 @@ int ref_synthetic_params(const ref_synthetic_config* config, int grid, isp_param
     out->auto_exposure.max_gain = p.auto_exposure.max_gain;
   });
 }
+
+
+#ifdef ISP_REF_CUDA
+// The reference's own CUDA backend, IspPipeline(Backend::kCuda)
+// (modules/isp/src/isp_pipeline.cpp, cuda_pipeline.cu), built for sm_100a
+// into oracle/_ref/libisp_ref_cuda.so: the GPU bar the B200 build is timed
+// against. Device buffers; frames queued on `stream`.
+__attribute__((visibility("default"))) void* ref_cuda_pipeline_create(const isp_params_c* params) {
+  void* handle = nullptr;
+  const int status = guarded([&] { handle = new isp::IspPipeline(isp::Backend::kCuda, to_params(*params)); });
+  return status == 0 ? handle : nullptr;
+}
+
+__attribute__((visibility("default"))) void ref_cuda_pipeline_destroy(void* handle) {
+  delete static_cast<isp::IspPipeline*>(handle);
+}
+
+__attribute__((visibility("default"))) int ref_cuda_pipeline_process(void* handle, const isp_raw_view_c* raw,
+                                                                    const isp_rgb_view_c* out, const isp_stats_c* stats,
+                                                                    const isp_exposure_c* exposure, void* stream) {
+  auto* p = static_cast<isp::IspPipeline*>(handle);
+  return guarded([&] {
+    const isp::RgbImageView rgb{out->data, out->pitch, static_cast<isp::OutputFormat>(out->format)};
+    isp::StatsOutput so{};
+    if (stats != nullptr) so = isp::StatsOutput{stats->histogram, stats->stats};
+    isp::FrameExposure fe{};
+    if (exposure != nullptr) fe = isp::FrameExposure{exposure->exposure_ns, exposure->gain};
+    p->process(to_raw(*raw), rgb, so, fe, static_cast<cudaStream_t>(stream));
+  });
+}
+#endif
 
 }  // extern "C"
