@@ -501,6 +501,17 @@ def run_b200(args):
         frames, secs, kind = cpu_throughput(w, raw, args.cpu_seconds, threads)
         cpu = {"value": frames * w.pixels / secs / 1e9, "unit": "Gpix/s", "cores": threads, "kind": kind,
                "sample": f"{frames} frames of {w.width}x{w.height} over {secs:.1f} s on {threads} threads"}
+        # One thread, the mean of 5 frames after 1 warm-up, as the reference's
+        # benchmark times its CPU backend (modules/isp/tests/benchmark.cpp:147-165).
+        make, _ = cpu_pipeline_factory()
+        single = make(w.params)
+        single.process(raw, w.out_format, w.with_stats)
+        t0 = time.perf_counter()
+        for _ in range(5):
+            single.process(raw, w.out_format, w.with_stats)
+        per_frame = (time.perf_counter() - t0) / 5
+        cpu["single_thread"] = {"value": w.pixels / per_frame / 1e9, "unit": "Gpix/s", "ms_per_frame": per_frame * 1e3,
+                                "sample": "1 thread, mean of 5 frames after 1 warm-up"}
 
     if dist is not None:
         dist.barrier()
