@@ -288,7 +288,7 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
   const size_t with_lut = main_kernel_smem(sharpen, d.raw_format, d.tone_size);
   int lut_in_smem = d.tone_size <= kLutSmemEntries && with_lut <= kSmemPerTwoCtas ? 1 : 0;
   const size_t need = lut_in_smem ? with_lut : without_lut;
-  const void* k = main_kernel(malvar, sharpen, pattern, lut_in_smem != 0);
+  const void* k = main_kernel(malvar, sharpen, pattern, lut_in_smem != 0, d.out_format);
   // The instance's attribute covers its largest footprint (uint16 boxes, a
   // full shared tone table), so frames of any format can share it.
   const size_t most = main_kernel_smem(sharpen, kRawU16, lut_in_smem ? kLutSmemEntries : 0);

@@ -6,21 +6,23 @@
 
 namespace isp_b200 {
 
-const void* main_kernel_bn(int layout, bool lut_smem);
-const void* main_kernel_bs(int layout, bool lut_smem);
-const void* main_kernel_mn(int layout, bool lut_smem);
-const void* main_kernel_ms(int layout, bool lut_smem);
+const void* main_kernel_bn(int layout, bool lut_smem, int out_format);
+const void* main_kernel_bs(int layout, bool lut_smem, int out_format);
+const void* main_kernel_mn(int layout, bool lut_smem, int out_format);
+const void* main_kernel_ms(int layout, bool lut_smem, int out_format);
 const void* batch_kernel_shared_lut();
 const void* batch_kernel_global_lut();
 
 const void* batch_kernel(bool lut_smem) { return lut_smem ? batch_kernel_shared_lut() : batch_kernel_global_lut(); }
 
-const void* main_kernel(bool malvar, bool sharpen, int pattern, bool lut_smem) {
+const void* main_kernel(bool malvar, bool sharpen, int pattern, bool lut_smem, int out_format) {
   // RGGB and BGGR share a layout (red/blue on the quad's diagonal), as do
   // GRBG and GBRG; the kernel swaps red and blue for BGGR and GBRG.
   const int layout = pattern >> 1;
-  if (malvar) return sharpen ? main_kernel_ms(layout, lut_smem) : main_kernel_mn(layout, lut_smem);
-  return sharpen ? main_kernel_bs(layout, lut_smem) : main_kernel_bn(layout, lut_smem);
+  if (malvar) {
+    return sharpen ? main_kernel_ms(layout, lut_smem, out_format) : main_kernel_mn(layout, lut_smem, out_format);
+  }
+  return sharpen ? main_kernel_bs(layout, lut_smem, out_format) : main_kernel_bn(layout, lut_smem, out_format);
 }
 
 size_t main_kernel_smem(bool sharpen, int raw_format, int lut_entries) {

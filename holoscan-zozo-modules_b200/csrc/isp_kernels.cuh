@@ -13,7 +13,7 @@ namespace isp_b200 {
 // (const CUtensorMap raw_map, FrameDesc, int tiles_x, int tiles, int use_tma,
 // int lut_in_smem). The raw map's box is main_box_row_bytes() bytes (or half
 // as many uint16 samples) by main_box_rows() rows.
-const void* main_kernel(bool malvar, bool sharpen, int pattern, bool lut_smem);
+const void* main_kernel(bool malvar, bool sharpen, int pattern, bool lut_smem, int out_format);
 size_t main_kernel_smem(bool sharpen, int raw_format, int lut_entries);
 int main_box_rows(bool sharpen);
 int main_box_row_bytes(int raw_format);

@@ -124,7 +124,7 @@ __device__ __forceinline__ void unit_rc(int u, bool same_parity, int& r, int& uc
 // is waited for on `bar`); after phase A, when the box is free again,
 // `after_a()` runs (to prefetch the next tile). Adds the tile's statistics
 // sums and saturated count to `acc` (per thread).
-template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, class AfterA>
+template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, class AfterA, int kOutSel = -1>
 __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f, const TileSmem& m, int* minmax,
                                          int x0, int y0, bool use_tma, uint64_t* bar, uint32_t& phase,
                                          u64 (&acc)[4], AfterA after_a) {
@@ -214,12 +214,24 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
     if (y < p.height) {
       const int nl = min(max(p.width - x, 0), 4);
       const int nr = min(max(p.width - x - kHalf, 0), 4);
+      // kOutSel: the output format fixed at compile time (the single-frame
+      // kernels), or -1 to choose it per unit (the batch kernel).
       if (nl == 4 && nr == 4 && p.out_vector) {
-        finish_pairs_any<kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist,
-                                         sums, npix);
+        if constexpr (kOutSel < 0) {
+          finish_pairs_any<kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist,
+                                           sums, npix);
+        } else {
+          finish_pairs<kOutSel, kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
+                                                m.hist, sums, npix);
+        }
       } else {
-        finish_pairs_any<kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist,
-                                          sums, npix);
+        if constexpr (kOutSel < 0) {
+          finish_pairs_any<kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
+                                            m.hist, sums, npix);
+        } else {
+          finish_pairs<kOutSel, kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
+                                                 m.hist, sums, npix);
+        }
       }
     }
   }
@@ -271,7 +283,7 @@ __device__ void flush_frame(const FrameDesc& p, const FrameSetup& f, const u64 (
   if (tid == 0) sc->main_done = 0;
 }
 
-template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem>
+template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, int kOut>
 __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_constant__ CUtensorMap map, FrameDesc p,
                                                                int tiles_x, int tiles, int use_tma, int lut_in_smem) {
   using G = Geom<kSharpen>;
@@ -321,21 +333,33 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
         issue(tile + gridDim.x);
       }
     };
-    run_tile<kMalvar, kSharpen, kLayout, kLutSmem>(p, f, m, minmax, x0, ty * kTH, use_tma != 0, &bar, phase, acc,
-                                                   prefetch);
+    run_tile<kMalvar, kSharpen, kLayout, kLutSmem, decltype(prefetch), kOut>(p, f, m, minmax, x0, ty * kTH,
+                                                                             use_tma != 0, &bar, phase, acc, prefetch);
     ++done;
   }
   flush_frame(p, f, acc, m.hist, red, &last, done, static_cast<unsigned int>(tiles));
 }
 
-template <bool kMalvar, bool kSharpen>
-const void* main_instance(int layout, bool lut_smem) {
+template <bool kMalvar, bool kSharpen, int kOut>
+const void* main_instance_out(int layout, bool lut_smem) {
   if (layout == 0) {
-    return lut_smem ? reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 0, true>)
-                    : reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 0, false>);
+    return lut_smem ? reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 0, true, kOut>)
+                    : reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 0, false, kOut>);
   }
-  return lut_smem ? reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 1, true>)
-                  : reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 1, false>);
+  return lut_smem ? reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 1, true, kOut>)
+                  : reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 1, false, kOut>);
+}
+
+// The tile kernel for a layout, tone-table placement and output format (one
+// instance per format, so that each holds only its own store code).
+template <bool kMalvar, bool kSharpen>
+const void* main_instance(int layout, bool lut_smem, int out_format) {
+  switch (out_format) {
+    case kOutRgb8: return main_instance_out<kMalvar, kSharpen, kOutRgb8>(layout, lut_smem);
+    case kOutRgba8: return main_instance_out<kMalvar, kSharpen, kOutRgba8>(layout, lut_smem);
+    case kOutRgb16: return main_instance_out<kMalvar, kSharpen, kOutRgb16>(layout, lut_smem);
+    default: return main_instance_out<kMalvar, kSharpen, kOutRgb32f>(layout, lut_smem);
+  }
 }
 
 }  // namespace

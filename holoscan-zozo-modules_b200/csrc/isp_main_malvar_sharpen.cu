@@ -3,8 +3,8 @@
 
 namespace isp_b200 {
 
-const void* main_kernel_ms(int layout, bool lut_smem) {
-  return main_instance<true, true>(layout, lut_smem);
+const void* main_kernel_ms(int layout, bool lut_smem, int out_format) {
+  return main_instance<true, true>(layout, lut_smem, out_format);
 }
 
 }  // namespace isp_b200

@@ -123,7 +123,7 @@ cudaError_t launch_noalloc(const FrameDesc& d, const isp_params_c& p, int sm_cou
   const size_t with_lut = main_kernel_smem(sharpen, d.raw_format, d.tone_size);
   int lut_in_smem = d.tone_size <= kLutSmemEntries && with_lut <= kSmemPerTwoCtas ? 1 : 0;
   const size_t need = lut_in_smem ? with_lut : main_kernel_smem(sharpen, d.raw_format, 0);
-  const void* k = main_kernel(p.demosaic == ISP_DEMOSAIC_MALVAR, sharpen, d.pattern, lut_in_smem != 0);
+  const void* k = main_kernel(p.demosaic == ISP_DEMOSAIC_MALVAR, sharpen, d.pattern, lut_in_smem != 0, d.out_format);
   const size_t most = main_kernel_smem(sharpen, kRawU16, lut_in_smem ? kLutSmemEntries : 0);
   int bpsm = 0;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(most));
