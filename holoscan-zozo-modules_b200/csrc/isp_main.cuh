@@ -65,11 +65,30 @@ struct FrameSetup {
   bool want_stats;
 };
 
-// Reads the frame's gains (its estimate, for auto white balance), copies the
-// tone table to shared memory (kLutSmem) and clears the block histogram.
-// The caller synchronises the block before the first tile.
+// The frame's shared-memory copies: the lens shading gains (when they fit),
+// the tone table (kLutSmem) and the cleared block histogram. They read only
+// the pipeline's own tables, never what the statistics pass writes.
 template <bool kLutSmem>
+__device__ __forceinline__ void fill_frame_smem(const FrameDesc& p, const TileSmem& m) {
+  const int gains = p.lsc_width * p.lsc_height * p.lsc_channels;
+  if (p.lsc != nullptr && gains <= kGridSmemGains) {
+    for (int i = threadIdx.x; i < gains; i += kThreads) m.grid[i] = p.lsc[i];
+  }
+  if constexpr (kLutSmem) {
+    for (int i = threadIdx.x; i < p.tone_size; i += kThreads) m.lut_s[i] = p.tone[i];
+  }
+  if (p.hist_out != nullptr) {
+    for (int i = threadIdx.x; i < kHistChannels * kHistBins; i += kThreads) m.hist[i] = 0U;
+  }
+}
+
+// Reads the frame's gains (its estimate, for auto white balance) and, with
+// kFill, fills the frame's shared memory (fill_frame_smem; without it the
+// caller did so before). The caller synchronises the block before the first
+// tile.
+template <bool kLutSmem, bool kFill = true>
 __device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const TileSmem& m) {
+  if constexpr (kFill) fill_frame_smem<kLutSmem>(p, m);
   FrameSetup f;
 #pragma unroll
   for (int k = 0; k < 3; ++k) f.gains[k] = p.auto_wb ? __ldcg(&p.scratch->awb_gains[k]) : p.wb[k];
@@ -80,17 +99,9 @@ __device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const Tile
     f.qinv[k] = p.inv_range[ch];
     f.qgain[k] = f.gains[color_of(ch)];
   }
-  f.grid = p.lsc;
   const int gains = p.lsc_width * p.lsc_height * p.lsc_channels;
-  if (p.lsc != nullptr && gains <= kGridSmemGains) {
-    for (int i = threadIdx.x; i < gains; i += kThreads) m.grid[i] = p.lsc[i];
-    f.grid = m.grid;
-  }
-  f.lut = p.tone;
-  if constexpr (kLutSmem) {
-    for (int i = threadIdx.x; i < p.tone_size; i += kThreads) m.lut_s[i] = p.tone[i];
-    f.lut = m.lut_s;
-  }
+  f.grid = p.lsc != nullptr && gains <= kGridSmemGains ? m.grid : p.lsc;
+  f.lut = kLutSmem ? m.lut_s : p.tone;
   f.lut_scale = static_cast<float>(p.tone_size - 1);
   // The demosaic runs as the layout's canonical pattern (RGGB or GRBG); for
   // BGGR and GBRG its red and blue outputs trade places before the colour
@@ -98,9 +109,6 @@ __device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const Tile
   f.swap_rb = (p.pattern & 1) != 0;
   f.want_hist = p.hist_out != nullptr;
   f.want_stats = p.stats_out != nullptr;
-  if (f.want_hist) {
-    for (int i = threadIdx.x; i < kHistChannels * kHistBins; i += kThreads) m.hist[i] = 0U;
-  }
   return f;
 }
 
@@ -311,13 +319,14 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
     fence_async_shared();
     if (static_cast<int>(blockIdx.x) < tiles) issue(blockIdx.x);
   }
+  fill_frame_smem<kLutSmem>(p, m);
   // Launched as a programmatic dependent of the statistics pass, this kernel
   // becomes resident on the SMs that pass leaves while it finishes; the wait
   // returns once the pass has completed and its writes (the gains that
   // setup_frame reads) are visible. Without a programmatic launch it returns
   // at once.
   griddep_wait();
-  const FrameSetup f = setup_frame<kLutSmem>(p, m);
+  const FrameSetup f = setup_frame<kLutSmem, false>(p, m);
   __syncthreads();
 
   u64 acc[4] = {0, 0, 0, 0};  // linear R, G, B in 2^-20 units; saturated samples
