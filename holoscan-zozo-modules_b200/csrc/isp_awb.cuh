@@ -31,7 +31,10 @@ __device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box,
   const int quads_x = p.width / 2;
   const int quads_y = p.height / 2;
   const unsigned int white = static_cast<unsigned int>(p.white);
-  for (int unit = threadIdx.x; unit < 512; unit += kThreads) {
+  static_assert(512 % kThreads == 0, "a tile's units split evenly over the block");
+#pragma unroll
+  for (int it = 0; it < 512 / kThreads; ++it) {
+    const int unit = static_cast<int>(threadIdx.x) + it * kThreads;
     const int a = unit >> 4;
     const int u = unit & 15;
     const int qy = (y0 >> 1) + a;
