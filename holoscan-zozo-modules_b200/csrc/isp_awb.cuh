@@ -31,6 +31,7 @@ __device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box,
   const int quads_x = p.width / 2;
   const int quads_y = p.height / 2;
   const unsigned int white = static_cast<unsigned int>(p.white);
+  unsigned int counted = 0;  // quads summed by this call
   static_assert(512 % kThreads == 0, "a tile's units split evenly over the block");
 #pragma unroll
   for (int it = 0; it < 512 / kThreads; ++it) {
@@ -125,9 +126,10 @@ __device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box,
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const float2 x = make_float2(fminf(v[k >> 1][k & 1].x, 4.0F), fminf(v[k >> 1][k & 1].y, 4.0F));
-      // to_fixed: trunc(x 2^20 + 0.5), the product exact.
+      // to_fixed: trunc(x 2^20 + 0.5), the product exact. Summed as 2^23
+      // bits + value; the 2^23 bits come off once, after the units.
       const float2 m = magic_trunc2(exact_scale_add2(x, bc2(kFixedOne), bc2(0.5F)));
-      sum[color_of(cfa_of(kPat, k))] += (ok0 ? magic_int(m.x) : 0U) + (ok1 ? magic_int(m.y) : 0U);
+      sum[color_of(cfa_of(kPat, k))] += (ok0 ? __float_as_uint(m.x) : 0U) + (ok1 ? __float_as_uint(m.y) : 0U);
       if constexpr (kWhitePatch) {
         // trunc(x 1024): an exact product, so its two-lane truncation is safe.
         const float2 b = magic_trunc2(mul2(x, bc2(static_cast<float>(kAwbBins))));
@@ -137,8 +139,14 @@ __device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box,
         if (ok1) atomicAdd(&h[b1 < kAwbBins - 1 ? b1 : kAwbBins - 1], 1U);
       }
     }
-    quads += (ok0 ? 1U : 0U) + (ok1 ? 1U : 0U);
+    counted += (ok0 ? 1U : 0U) + (ok1 ? 1U : 0U);
   }
+  // Every counted quad added one red, two green and one blue sample, each
+  // with 2^23 bits on top (sums mod 2^32; the true sums fit 32 bits).
+  sum[0] -= counted * kTwo23Bits;
+  sum[1] -= 2U * counted * kTwo23Bits;
+  sum[2] -= counted * kTwo23Bits;
+  quads += counted;
 }
 
 template <int kSrc, bool kWhitePatch, int kPat>
