@@ -275,7 +275,10 @@ def workload_config(w: scene.Workload, nbuf: int = 0):
            "bit_depth": w.bits, "output": ["RGB8", "RGBA8", "RGB16", "RGB32F"][w.out_format],
            "white_balance": ["manual", "gray-world", "white-patch"][w.params.white_balance],
            "demosaic": ["bilinear", "malvar"][w.params.demosaic], "sharpen": w.params.sharpen,
-           "histogram": w.with_hist, "stats": w.with_stats, "compulsory_bytes_per_frame": w.compulsory_bytes()}
+           # The reference's histogram output is [4][256] (luma, R, G, B of the
+           # 8-bit codes of the stored image); it has no 1024-bin form.
+           "histogram": "[4][256] of the 8-bit output codes" if w.with_hist else False,
+           "stats": w.with_stats, "compulsory_bytes_per_frame": w.compulsory_bytes()}
     if w.fresh_frames:
         cfg["frames"] = (f"{w.fresh_frames} fresh-seed frames rendered on the device (isp_b200_synthetic_raw), "
                          f"taken in turn: {w.fresh_frames * abi.raw_row_bytes(w.fmt, w.width) * w.height / 1e9:.1f} GB "
