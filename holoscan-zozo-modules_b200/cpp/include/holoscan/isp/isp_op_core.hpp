@@ -18,6 +18,7 @@
 #include <atomic>
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <optional>
 #include <string>
 #include <utility>
@@ -76,6 +77,11 @@ struct ImageInput {
   unsigned significant_bits{};  // 0 (or kUnknownSignificantBits) unknown
   std::int64_t exposure_time_ns{};
   float gain{};
+  // For pinned host memory: keeps the tensor's memory from reuse until the
+  // work queued on the stream so far is done (the SDK's
+  // Tensor::set_deallocation_stream); false when the tensor cannot. Without
+  // it, or when it fails, the operator waits for the stream after the copy.
+  std::function<bool(cudaStream_t)> hold_until_done;
 };
 inline constexpr unsigned kUnknownSignificantBits = 0xFFFFFFFFU;
 
@@ -225,10 +231,14 @@ class IspOpCore {
   [[nodiscard]] const IspOpConfig& config() const noexcept { return config_; }
 
   // One received frame: described, staged into device memory when it
-  // arrived in host memory (pageable: the copy waits; pinned: queued, and the
-  // caller keeps the buffer until `stream` has passed the copy), and
-  // queued through the pipeline on `stream` into `image` (device memory,
-  // packed rows) and, with config().stats, `histogram` and `stats`.
+  // arrived in host memory, and queued through the pipeline on `stream` into
+  // `image` (device memory, packed rows) and, with config().stats,
+  // `histogram` and `stats`. Staging follows isp_op.cpp:392-441: a pageable
+  // frame is waited for (its producer) and its copy returns once staged (a
+  // second wait); a pinned frame's copy is queued, and its memory is kept
+  // from reuse until the stream has passed the copy, by the input's
+  // hold_until_done where it succeeds, else by waiting for the stream (one
+  // wait).
   // @throws std::invalid_argument with the operator's message for an unusable input.
   // @throws std::runtime_error if CUDA fails.
   ImageOutput process(const ImageInput& in, void* image, std::uint32_t* histogram, float* stats,
@@ -252,7 +262,13 @@ class IspOpCore {
       }
       check(cudaMemcpyAsync(staging_, f.view.data, f.span, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync");
       detail::g_op_copies.fetch_add(1, std::memory_order_relaxed);
-      if (in.memory == MemoryKind::kHost) count_wait();  // a pageable copy returns once staged
+      if (in.memory == MemoryKind::kHost) {
+        count_wait();  // a pageable copy returns once staged
+      } else if (!in.hold_until_done || !in.hold_until_done(stream)) {
+        // The producer must not reuse pinned memory while the copy reads it.
+        count_wait();
+        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+      }
       f.view.data = staging_;
     }
     last_stream_ = stream;

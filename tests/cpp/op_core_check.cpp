@@ -148,6 +148,18 @@ int gpu_checks() {
   in.data = pinned;
   core.process(in, outs[1], hist, st, nullptr);
   const IspOpStatistics s2 = isp_op_statistics();
+  // Pinned again, with a tensor that holds its memory until the stream has
+  // passed the copy (the SDK's set_deallocation_stream): no wait.
+  int holds = 0;
+  cudaStream_t held_on = reinterpret_cast<cudaStream_t>(1);
+  in.hold_until_done = [&](cudaStream_t s) {
+    ++holds;
+    held_on = s;
+    return true;
+  };
+  core.process(in, outs[1], hist, st, nullptr);
+  in.hold_until_done = nullptr;
+  const IspOpStatistics s2h = isp_op_statistics();
   in.memory = MemoryKind::kDevice;
   in.data = d_raw;
   core.process(in, outs[2], hist, st, nullptr);
@@ -164,14 +176,17 @@ int gpu_checks() {
     same = same && std::memcmp(a.data(), b.data(), out_bytes) == 0;
   }
   std::printf("{\"check\": \"gpu\", \"error\": \"%s\", \"same\": %d, \"pageable_waits\": %llu, \"pageable_copies\": %llu, "
-              "\"pinned_waits\": %llu, \"pinned_copies\": %llu, \"device_waits\": %llu, \"device_copies\": %llu}\n",
+              "\"pinned_waits\": %llu, \"pinned_copies\": %llu, \"held_waits\": %llu, \"held_copies\": %llu, "
+              "\"holds\": %d, \"held_on_stream\": %d, \"device_waits\": %llu, \"device_copies\": %llu}\n",
               cudaGetErrorString(cudaDeviceSynchronize()), same,
               static_cast<unsigned long long>(s1.host_waits - s0.host_waits),
               static_cast<unsigned long long>(s1.copies - s0.copies),
               static_cast<unsigned long long>(s2.host_waits - s1.host_waits),
               static_cast<unsigned long long>(s2.copies - s1.copies),
-              static_cast<unsigned long long>(s3.host_waits - s2.host_waits),
-              static_cast<unsigned long long>(s3.copies - s2.copies));
+              static_cast<unsigned long long>(s2h.host_waits - s2.host_waits),
+              static_cast<unsigned long long>(s2h.copies - s2.copies), holds, held_on == nullptr ? 1 : 0,
+              static_cast<unsigned long long>(s3.host_waits - s2h.host_waits),
+              static_cast<unsigned long long>(s3.copies - s2h.copies));
   for (auto& o : outs) cudaFree(o);
   cudaFree(d_raw);
   cudaFreeHost(pinned);

@@ -158,8 +158,13 @@ def test_operator_describes_inputs_as_the_reference_does(op_core):
 def test_operator_stages_host_frames_and_counts_waits_and_copies(op_core):
     g = _checks(op_core, "gpu")["gpu"]
     assert g["error"] == "no error" and g["same"] == 1
-    # A pageable host frame: the producer's wait and the copy's wait, one copy;
-    # a pinned frame: one queued copy; a device frame: nothing.
+    # As the reference's operator test counts them (isp_op_test.cpp:220-232,
+    # README's table): a pageable host frame waits for its producer and for
+    # the staged copy, one copy; a pinned frame whose tensor cannot hold its
+    # memory waits once for the copy; a device frame costs nothing.
     assert (g["pageable_waits"], g["pageable_copies"]) == (2, 1)
-    assert (g["pinned_waits"], g["pinned_copies"]) == (0, 1)
+    assert (g["pinned_waits"], g["pinned_copies"]) == (1, 1)
+    # A pinned frame whose tensor holds its memory until the stream passes
+    # the copy (set_deallocation_stream): the hold on the operator's stream, no wait.
+    assert (g["held_waits"], g["held_copies"], g["holds"], g["held_on_stream"]) == (0, 1, 1, 1)
     assert (g["device_waits"], g["device_copies"]) == (0, 0)
