@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_kernel(const __grid_const
       issue(ty + 1, buf ^ 1);
     }
     if (use_tma && !mbar_wait(&bars[buf], (phases >> buf) & 1U)) {
-      if (tid == 0) atomicExch(&s->error, 1);
+      if (tid == 0) report_wait_timeout(s);
     }
     phases ^= 1U << buf;
     const uint8_t* box = boxes + buf * 64 * 128;

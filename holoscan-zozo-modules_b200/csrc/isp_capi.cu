@@ -485,6 +485,26 @@ int isp_b200_device_status(isp_b200_pipeline* pl, int32_t* status) {
   return ISP_OK;
 }
 
+int isp_b200_check_bounded_wait(isp_b200_pipeline* pl, uint32_t polls, void* stream_ptr) {
+  if (pl == nullptr) return fail(ISP_EINVAL, "pipeline is null");
+  if (polls == 0U || polls > (1U << 20)) return fail(ISP_EINVAL, "polls must be 1..1048576");
+  auto stream = static_cast<cudaStream_t>(stream_ptr);
+  static_cast<void>(cudaGetLastError());
+  cudaError_t error = cudaSuccess;
+  if (pl->queued) error = cudaStreamWaitEvent(stream, pl->done, 0);
+  if (error == cudaSuccess) {
+    Scratch* scratch = pl->state.scratch;
+    unsigned int n = polls;
+    void* args[] = {&scratch, &n};
+    error = cudaLaunchKernel(wait_check_kernel(), dim3(1), dim3(32), args, 0, stream);
+  }
+  if (error == cudaSuccess) error = cudaEventRecord(pl->done, stream);
+  if (error != cudaSuccess) return fail_cuda(error, "isp_b200_check_bounded_wait");
+  pl->queued = true;
+  clear_error();
+  return ISP_OK;
+}
+
 int isp_b200_set_kernel_events(isp_b200_pipeline* pl, void* before, void* after) {
   if (pl == nullptr) return fail(ISP_EINVAL, "pipeline is null");
   pl->before_main = static_cast<cudaEvent_t>(before);

@@ -6,6 +6,27 @@
 
 namespace isp_b200 {
 
+namespace {
+
+// The bounded wait of the tile and statistics passes, made to run out: one
+// thread announces bytes on a barrier that no copy will ever complete, every
+// thread waits `polls` times, gives up, and the pipeline's error flag is set
+// as a real pass sets it. No copy is issued, so nothing is in flight when
+// the kernel returns.
+__global__ void isp_wait_check_kernel(Scratch* scratch, unsigned int polls) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&bar)), "r"(16U) : "memory");
+  }
+  __syncthreads();
+  if (!mbar_wait(&bar, 0, polls) && threadIdx.x == 0) report_wait_timeout(scratch);
+}
+
+}  // namespace
+
+const void* wait_check_kernel() { return reinterpret_cast<const void*>(&isp_wait_check_kernel); }
+
 const void* main_kernel_bn(int layout, bool lut_smem, int out_format);
 const void* main_kernel_bs(int layout, bool lut_smem, int out_format);
 const void* main_kernel_mn(int layout, bool lut_smem, int out_format);

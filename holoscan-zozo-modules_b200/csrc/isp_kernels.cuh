@@ -32,6 +32,11 @@ int awb_kernel_tiles(int width, int height, int* tiles_x);
 // returns the CTA count (strips x bands).
 int awb_kernel_bands(int width, int height, int ctas, int* strips, int* tiles_y, int* band_tiles);
 
+// The bounded-wait check (arguments Scratch*, unsigned int polls; one CTA):
+// a barrier nothing completes, waited for `polls` times, then the pipeline's
+// error flag set as a pass that gave up sets it.
+const void* wait_check_kernel();
+
 // Tone tables up to this many entries may be copied into shared memory.
 constexpr int kLutSmemEntries = 4097;
 // In a batch, tone tables up to this many entries go to shared memory.

@@ -70,6 +70,7 @@ def lib() -> C.CDLL:
                                                P(abi.ExposureC), C.c_void_p]
         L.isp_b200_device_status.argtypes = [C.c_void_p, P(C.c_int32)]
         L.isp_b200_set_kernel_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.isp_b200_check_bounded_wait.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
         L.isp_b200_process_host.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
                                             P(abi.ExposureC)]
         L.isp_b200_batch_create.argtypes = [C.c_int32, P(C.c_void_p)]
@@ -194,6 +195,11 @@ class Pipeline:
         v = C.c_int32()
         check(lib().isp_b200_device_status(self.handle, C.byref(v)))
         return int(v.value)
+
+    def check_bounded_wait(self, polls: int = 1024, stream: int = 0) -> None:
+        """Queues a kernel whose bounded barrier wait runs out after `polls` polls and flags this camera
+        as a pass that gave up a wait does (device_status then reads 1 once)."""
+        check(lib().isp_b200_check_bounded_wait(self.handle, polls, stream or None))
 
     def set_kernel_events(self, before: int = 0, after: int = 0) -> None:
         """Events (cudaEvent_t handles) recorded around the fused tile kernel of every later frame."""

@@ -413,6 +413,14 @@ ISP_B200_API int isp_b200_process_noalloc(const isp_params_c* params, const isp_
  * trustworthy), else 0. */
 ISP_B200_API int isp_b200_device_status(isp_b200_pipeline* pipeline, int32_t* status);
 
+/* Check of the bounded device waits, no reference counterpart: queues on
+ * `stream`, ordered after the pipeline's frames, one kernel that waits on a
+ * barrier no copy ever completes, gives up after `polls` polls (1..2^20) and
+ * flags the pipeline as a tile or statistics pass that gave up a wait flags
+ * it; isp_b200_device_status then reports 1 once. Nothing is left in flight
+ * and the pipeline's next frame is unaffected. */
+ISP_B200_API int isp_b200_check_bounded_wait(isp_b200_pipeline* pipeline, uint32_t polls, void* stream);
+
 /* Profiling hook, no reference counterpart: events (cudaEvent_t, may be null)
  * that every following process call records on its stream right before and
  * right after the fused tile kernel, so a caller can time that kernel alone. */

@@ -153,3 +153,24 @@ def test_config2_8k_raw12_matches_oracle():
     assert same_bits(got.image, exp.image), first_mismatch(got.image, exp.image)
     assert np.array_equal(got.histogram, exp.histogram)
     assert same_bits(got.stats, exp.stats)
+
+
+def test_a_bounded_wait_that_runs_out_is_reported_and_the_next_frame_is_clean():
+    """The kernels' barrier waits are bounded: a wait that runs out returns,
+    flags the camera (isp_b200_device_status reads 1 once), and leaves the
+    context and the pipeline usable. The check kernel waits on a barrier that
+    no copy completes; no GPU fault is involved."""
+    torch = torch_cuda()
+    case = load_case("malvar_gray_world")
+    pipe = isp_b200.Pipeline(case.params)
+    stream = torch.cuda.Stream()
+    pipe.check_bounded_wait(256, stream.cuda_stream)
+    assert pipe.device_status() == 1
+    assert pipe.device_status() == 0, "the status is cleared once read"
+    for f, raw in enumerate(case.frame_raws()):
+        got = run_device(pipe, raw, case.out_format, case.with_stats, case.exposure)
+        _check("malvar_gray_world", f, got, case.expected[f], case.with_stats)
+    assert pipe.device_status() == 0
+    with pytest.raises(ValueError, match="polls must be"):
+        pipe.check_bounded_wait(0)
+    pipe.close()
