@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(kThreads, 2) isp_batch_kernel(const BatchFrame
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
   const TileSmem m = carve(smem, layout_of(true, box_row_bytes(kRawU16), kLutSmem ? kBatchLutEntries : 0), GS::kSH);
   __shared__ uint64_t bar;
-  __shared__ u64 red[kWarps];
+  __shared__ u64 red[4 * kWarps];
   __shared__ int minmax[2];
   __shared__ bool last;
   __shared__ __align__(16) FrameDesc fd;
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_batch_kernel(const BatchF
   float* row_ty = reinterpret_cast<float*>(row_k + 64);
   unsigned int* hist = reinterpret_cast<unsigned int*>(row_ty + 64);      // [3][1024]
   __shared__ uint64_t bars[2];
-  __shared__ u64 red[kWarps];
+  __shared__ u64 red[4 * kWarps];
   __shared__ int minmax[2];
   __shared__ int first;
   __shared__ bool last;
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_batch_kernel(const BatchF
                                  row_ty, table, minmax);
     const bool use_tma = bf.use_tma != 0;
     if (use_tma) {
-      if (!mbar_wait(&bars[buf], (phases >> buf) & 1U) && tid == 0) atomicExch(&fd.scratch->error, 1);
+      if (!mbar_wait(&bars[buf], (phases >> buf) & 1U) && tid == 0) report_wait_timeout(fd.scratch);
       phases ^= 1U << buf;
     }
     float black[4], inv[4];

@@ -6,6 +6,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 
 #include "isp_device.cuh"
@@ -157,9 +158,9 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, void* dst, u
       : "memory");
 }
 
-// Waits for the barrier's phase `parity` to complete; false after kWaitLimit polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (unsigned int i = 0; i < kWaitLimit; ++i) {
+// Waits for the barrier's phase `parity` to complete; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int limit = kWaitLimit) {
+  for (unsigned int i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
@@ -170,6 +171,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   }
   return false;
 }
+
+// A bounded wait gave up: the frame's outputs are not trustworthy. The flag
+// stays set until isp_b200_device_status reads and clears it.
+__device__ __forceinline__ void report_wait_timeout(Scratch* s) { atomicExch(&s->error, 1); }
 
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
@@ -352,6 +357,26 @@ __device__ u64 block_sum(u64 v, u64* red) {
 #pragma unroll
   for (int w = 0; w < kWarps; ++w) total += red[w];
   return total;
+}
+
+// Sums of four u64 per thread over the block, in `out` of thread 0; `red`
+// holds 4 x kWarps values.
+__device__ __forceinline__ void block_sum4(const u64 (&v)[4], u64* red, u64 (&out)[4]) {
+  u64 w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) w[k] = warp_sum(v[k]);
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) red[k * kWarps + (threadIdx.x >> 5)] = w[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    u64 total = 0;
+#pragma unroll
+    for (int i = 0; i < kWarps; ++i) total += red[k * kWarps + i];
+    out[k] = total;
+  }
 }
 
 // Exclusive prefix sum of one u64 per thread over the block.

@@ -120,6 +120,17 @@ __device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const Tile
 // different banks. Without sharpening a warp keeps one row parity (the
 // Bayer sites are compile-time) and the rows are r and r + 2, which the
 // sample plane's swizzle (psw) sends to different banks.
+// With sharpening, thread t takes output rows r and r + 1 (r even) of group
+// uc: a warp covers 8 rows x 8 groups, and each quarter-warp groups 0..3 or
+// 4..7 of two neighbouring row pairs (the RGB planes' swizzle, csw, sends
+// them to different banks).
+__device__ __forceinline__ void unit_rows2(int t, int& r, int& uc) {
+  const int w = t >> 5;
+  const int l = t & 31;
+  uc = (l & 3) | (((l >> 3) & 1) << 2);
+  r = 8 * w + 2 * (((l >> 2) & 1) + ((l >> 4) << 1));
+}
+
 __device__ __forceinline__ void unit_rc(int u, bool same_parity, int& r, int& uc) {
   const int w = u >> 5;
   const int l = u & 31;
@@ -155,7 +166,7 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
                          p.height + G::kHalo - 1, m.col_mx, m.col_ix, m.col_tx, m.row_my, m.row_k, m.row_ty,
                          reinterpret_cast<float*>(m.table), minmax);
   if (use_tma) {
-    if (!mbar_wait(bar, phase) && tid == 0) atomicExch(&p.scratch->error, 1);
+    if (!mbar_wait(bar, phase) && tid == 0) report_wait_timeout(p.scratch);
     phase ^= 1U;
   }
 
@@ -179,30 +190,72 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
     __syncthreads();
   }
 
-  // C. Two units of four pairs of one row per thread. The statistics sums
-  //    stay below 2^32 per thread and tile (16 pixels of at most 2^20).
+  // C. The per-pixel tail of four pairs of one row (x .. x + 3 and
+  //    x + 32 .. x + 35). The statistics sums stay below 2^32 per thread and
+  //    tile (16 pixels of at most 2^20).
   unsigned int sums[3] = {0U, 0U, 0U};
   unsigned int npix = 0;
-  const float2 amount = bc2(p.sharpen);
-#pragma unroll 1
-  for (int k = 0; k < 2; ++k) {
-    const int unit = tid + k * kThreads;
-    int r, uc;
-    float2 rgb[4][3];
-    if constexpr (kSharpen) {
-      unit_rc(unit, false, r, uc);
-      float2 ch[4];
-      sharpen_row4(m.R, r, uc, amount, ch);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) rgb[i][0] = ch[i];
-      sharpen_row4(m.G, r, uc, amount, ch);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) rgb[i][1] = ch[i];
-      sharpen_row4(m.B, r, uc, amount, ch);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) rgb[i][2] = ch[i];
+  const auto finish_row = [&](const float2 (&rgb)[4][3], int r, int uc) {
+    const int x = x0 + 4 * uc;
+    const int y = y0 + r;
+    if (y >= p.height) return;
+    const int nl = min(max(p.width - x, 0), 4);
+    const int nr = min(max(p.width - x - kHalf, 0), 4);
+    // kOutSel: the output format fixed at compile time (the single-frame
+    // kernels), or -1 to choose it per unit (the batch kernel).
+    if (nl == 4 && nr == 4 && p.out_vector) {
+      if constexpr (kOutSel < 0) {
+        finish_pairs_any<kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist,
+                                         sums, npix);
+      } else {
+        finish_pairs<kOutSel, kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
+                                              m.hist, sums, npix);
+      }
     } else {
-      unit_rc(unit, true, r, uc);
+      if constexpr (kOutSel < 0) {
+        finish_pairs_any<kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist,
+                                          sums, npix);
+      } else {
+        finish_pairs<kOutSel, kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
+                                               m.hist, sums, npix);
+      }
+    }
+  };
+  if constexpr (kSharpen) {
+    // One unit per thread: output rows r and r + 1 of group uc, whose RGB
+    // rows r .. r + 3 each plane loads once.
+    int r, uc;
+    unit_rows2(tid, r, uc);
+    const float2 amount = bc2(p.sharpen);
+    float2 rgb0[4][3], rgb1[4][3];
+    float2 o0[4], o1[4];
+    sharpen_rows2(m.R, r, uc, amount, o0, o1);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      rgb0[i][0] = o0[i];
+      rgb1[i][0] = o1[i];
+    }
+    sharpen_rows2(m.G, r, uc, amount, o0, o1);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      rgb0[i][1] = o0[i];
+      rgb1[i][1] = o1[i];
+    }
+    sharpen_rows2(m.B, r, uc, amount, o0, o1);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      rgb0[i][2] = o0[i];
+      rgb1[i][2] = o1[i];
+    }
+    finish_row(rgb0, r, uc);
+    finish_row(rgb1, r + 1, uc);
+  } else {
+    // Two units of four pairs of one row per thread, straight from the samples.
+#pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+      int r, uc;
+      unit_rc(tid + k * kThreads, true, r, uc);
+      float2 rgb[4][3];
       if (r & 1) {
         demosaic_row4<kMalvar, kPat, 1>(m.P, r, uc, rgb);
       } else {
@@ -216,31 +269,7 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
           rgb[i][2] = red;
         }
       }
-    }
-    const int x = x0 + 4 * uc;
-    const int y = y0 + r;
-    if (y < p.height) {
-      const int nl = min(max(p.width - x, 0), 4);
-      const int nr = min(max(p.width - x - kHalf, 0), 4);
-      // kOutSel: the output format fixed at compile time (the single-frame
-      // kernels), or -1 to choose it per unit (the batch kernel).
-      if (nl == 4 && nr == 4 && p.out_vector) {
-        if constexpr (kOutSel < 0) {
-          finish_pairs_any<kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist,
-                                           sums, npix);
-        } else {
-          finish_pairs<kOutSel, kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
-                                                m.hist, sums, npix);
-        }
-      } else {
-        if constexpr (kOutSel < 0) {
-          finish_pairs_any<kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
-                                            m.hist, sums, npix);
-        } else {
-          finish_pairs<kOutSel, kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
-                                                 m.hist, sums, npix);
-        }
-      }
+      finish_row(rgb, r, uc);
     }
   }
 #pragma unroll
@@ -251,23 +280,37 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
 // The main pass's flush of one frame by one CTA, after it processed
 // `tiles_done` of the frame's `tiles_total` tiles: block sums and histogram
 // into the frame's scratch; the CTA that completes the frame's tile count
-// writes the user's histogram and statistics and clears the scratch.
+// writes the user's histogram and statistics and clears the scratch (and
+// the tile claims of the single-frame pass). `red` holds 4 x kWarps values.
 __device__ void flush_frame(const FrameDesc& p, const FrameSetup& f, const u64 (&acc)[4], unsigned int* hist,
                             u64* red, bool* last, unsigned int tiles_done, unsigned int tiles_total) {
   Scratch* sc = p.scratch;
   const int tid = threadIdx.x;
-  if (!f.want_stats && !f.want_hist) return;
-  if (f.want_stats) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const u64 total = block_sum(acc[k], red);
-      if (tid == 0 && total != 0) atomicAdd(k < 3 ? &sc->sum[k] : &sc->saturated, total);
+  if (!f.want_stats && !f.want_hist) {
+    // Nothing to finish, but the last CTA still clears the counters.
+    __syncthreads();
+    if (tid == 0 && atomicAdd(&sc->main_done, tiles_done) + tiles_done == tiles_total) {
+      sc->main_done = 0;
+      sc->tile_next = 0;
     }
+    return;
+  }
+  if (f.want_stats) {
+    u64 total[4];
+    block_sum4(acc, red, total);
+    if (tid < 4 && total[tid] != 0) atomicAdd(tid < 3 ? &sc->sum[tid] : &sc->saturated, total[tid]);
   }
   if (f.want_hist) {
     __syncthreads();
-    for (int i = tid; i < kHistChannels * kHistBins; i += kThreads) {
-      if (hist[i] != 0U) atomicAdd(&sc->hist[i], hist[i]);
+    // Two bins per 64-bit atomic: a bin's count over a frame stays below
+    // 2^32, so no carry crosses into its neighbour.
+    static_assert(offsetof(Scratch, hist) % 8 == 0, "histogram pairs are 8-byte aligned");
+    for (int i = tid; i < kHistChannels * kHistBins / 2; i += kThreads) {
+      const uint2 h = reinterpret_cast<const uint2*>(hist)[i];
+      if ((h.x | h.y) != 0U) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(&sc->hist[2 * i]),
+                  (static_cast<unsigned long long>(h.y) << 32) | h.x);
+      }
     }
   }
   __threadfence();
@@ -288,7 +331,10 @@ __device__ void flush_frame(const FrameDesc& p, const FrameSetup& f, const u64 (
     sc->sum[0] = sc->sum[1] = sc->sum[2] = 0;
     sc->saturated = 0;
   }
-  if (tid == 0) sc->main_done = 0;
+  if (tid == 0) {
+    sc->main_done = 0;
+    sc->tile_next = 0;
+  }
 }
 
 template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, int kOut>
@@ -300,8 +346,9 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
   const int box_bytes = box_row_bytes(p.raw_format);
   const TileSmem m = carve(smem, layout_of(kSharpen, box_bytes, kLutSmem ? p.tone_size : 0), G::kSH);
   __shared__ uint64_t bar;
-  __shared__ u64 red[kWarps];
+  __shared__ u64 red[4 * kWarps];
   __shared__ int minmax[2];
+  __shared__ int next_tile;
   __shared__ bool last;
   static_cast<void>(lut_in_smem);
 
@@ -332,19 +379,30 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
   u64 acc[4] = {0, 0, 0, 0};  // linear R, G, B in 2^-20 units; saturated samples
   uint32_t phase = 0;
   unsigned int done = 0;
-  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+  // Tiles are claimed as CTAs free up: the first per CTA is its index, the
+  // rest come from the frame's counter, so CTAs that meet slower tiles
+  // (edges, mirrored borders) take fewer and all finish together.
+  int tile = blockIdx.x;
+  while (tile < tiles) {
     const int ty = tile / tiles_x;
     const int x0 = (tile - ty * tiles_x) * kTW;
-    // The box is free after phase A: prefetch the next tile during B and C.
+    // The CTA's next tile, claimed now; its box is requested once this
+    // tile's box is free (after phase A), to arrive during B and C.
+    unsigned int claim = 0;
+    if (threadIdx.x == 0) claim = gridDim.x + atomicAdd(&p.scratch->tile_next, 1U);
     const auto prefetch = [&] {
-      if (use_tma && threadIdx.x == 0 && tile + static_cast<int>(gridDim.x) < tiles) {
-        fence_async_shared();
-        issue(tile + gridDim.x);
+      if (threadIdx.x == 0) {
+        next_tile = static_cast<int>(claim);
+        if (use_tma && static_cast<int>(claim) < tiles) {
+          fence_async_shared();
+          issue(static_cast<int>(claim));
+        }
       }
     };
     run_tile<kMalvar, kSharpen, kLayout, kLutSmem, decltype(prefetch), kOut>(p, f, m, minmax, x0, ty * kTH,
                                                                              use_tma != 0, &bar, phase, acc, prefetch);
     ++done;
+    tile = next_tile;  // written before run_tile's closing barrier
   }
   flush_frame(p, f, acc, m.hist, red, &last, done, static_cast<unsigned int>(tiles));
 }

@@ -34,6 +34,14 @@ constexpr int kUnitsA = kPW / 4;  // phase A units per sample row: 4 pairs each
 // meets every bank once. Accesses are whole 16-byte chunks (even s).
 __device__ __forceinline__ int psw(int j) { return ((j >> 1) & 1) << 1; }
 
+// Bank spread of the RGB planes (rows of 17 16-byte chunks): chunk c < 16 of
+// row j sits at j * 17 + (c ^ csw(j)), rows 2k and 2k + 1 in order, rows
+// 2k + 2 and 2k + 3 with neighbouring chunks swapped (chunk 16, the ring,
+// stays), so that a quarter-warp reading four groups of each of two row
+// pairs (rows r + a and r + 2 + a) meets every bank once but for chunk 16.
+__device__ __forceinline__ int csw(int j) { return (j >> 1) & 1; }
+__device__ __forceinline__ int cchunk(int c, int sw) { return c < kCW2 / 2 - 1 ? c ^ sw : c; }
+
 __device__ __forceinline__ float4 lds4(const float2* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void sts4(float2* p, float2 a, float2 b) {
   *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
@@ -202,7 +210,7 @@ __device__ __forceinline__ void phase_b2(const float2* P, float2* R, float2* G, 
     }
 #pragma unroll
     for (int dy = 0; dy < 2; ++dy) {
-      const int o = (2 * ur + dy) * kCW2 + 2 * uq;
+      const int o = (2 * ur + dy) * kCW2 + 2 * cchunk(uq, ur & 1);  // csw(2 ur + dy) == ur & 1
       sts4(R + o, rgb[dy][0][0], rgb[dy][1][0]);
       sts4(G + o, rgb[dy][0][1], rgb[dy][1][1]);
       sts4(B + o, rgb[dy][0][2], rgb[dy][1][2]);
@@ -210,14 +218,20 @@ __device__ __forceinline__ void phase_b2(const float2* P, float2* R, float2* G, 
   }
 }
 
-// C (sharpening). The 3x3 window of one plane around pairs 4uc .. 4uc + 3 of
-// output row r, sharpened: RGB rows r .. r + 2, pair columns 4uc .. 4uc + 5.
-__device__ __forceinline__ void sharpen_row4(const float2* X, int r, int uc, float2 amount, float2 (&out)[4]) {
-  float2 w[3][6];
+// C (sharpening). The 3x3 windows of one plane around pairs 4uc .. 4uc + 3
+// of output rows r and r + 1, sharpened: RGB rows r .. r + 3 (each loaded
+// once for both output rows), pair columns 4uc .. 4uc + 5 (chunks 2uc ..
+// 2uc + 2, stored at chunk ^ csw(row)).
+__device__ __forceinline__ void sharpen_rows2(const float2* X, int r, int uc, float2 amount, float2 (&o0)[4],
+                                              float2 (&o1)[4]) {
+  float2 w[4][6];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float2* row = X + (r + a) * kCW2 + 4 * uc;
-    const float4 v0 = lds4(row), v1 = lds4(row + 2), v2 = lds4(row + 4);
+  for (int a = 0; a < 4; ++a) {
+    const int j = r + a;
+    const int s = csw(j);
+    const float2* row = X + j * kCW2;
+    const float4 v0 = lds4(row + 2 * ((2 * uc) ^ s)), v1 = lds4(row + 2 * ((2 * uc + 1) ^ s)),
+                 v2 = lds4(row + 2 * cchunk(2 * uc + 2, s));
     w[a][0] = lo2(v0);
     w[a][1] = hi2(v0);
     w[a][2] = lo2(v1);
@@ -227,8 +241,10 @@ __device__ __forceinline__ void sharpen_row4(const float2* X, int r, int uc, flo
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    out[i] = sharpen_one2(w[1][i + 1], w[0][i + 1], w[2][i + 1], w[1][i], w[1][i + 2], w[0][i], w[0][i + 2], w[2][i],
-                          w[2][i + 2], amount);
+    o0[i] = sharpen_one2(w[1][i + 1], w[0][i + 1], w[2][i + 1], w[1][i], w[1][i + 2], w[0][i], w[0][i + 2], w[2][i],
+                         w[2][i + 2], amount);
+    o1[i] = sharpen_one2(w[2][i + 1], w[1][i + 1], w[3][i + 1], w[2][i], w[2][i + 2], w[1][i], w[1][i + 2], w[3][i],
+                         w[3][i + 2], amount);
   }
 }
 

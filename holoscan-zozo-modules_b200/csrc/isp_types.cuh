@@ -40,7 +40,8 @@ struct Scratch {
   unsigned int hist[kHistChannels * kHistBins];
   unsigned int main_done;  // tiles of the main pass flushed so far
   int error;  // a bounded wait in a kernel gave up (1)
-  unsigned int pad[2];
+  unsigned int tile_next;  // the single-frame tile pass's tiles claimed beyond the first one per CTA
+  unsigned int pad;
 };
 
 struct AutoExposure {
