@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_kernel(const __grid_const
     acc[3] += quads;
     __syncthreads();
   }
-  awb_flush(p, acc, hist, kWhitePatch, red, &first, &last, static_cast<unsigned int>(ty1 > ty0 ? ty1 - ty0 : 0),
+  awb_flush<true>(p, acc, hist, kWhitePatch, red, &first, &last, static_cast<unsigned int>(ty1 > ty0 ? ty1 - ty0 : 0),
             static_cast<unsigned int>(strips * tiles_y));
 }
 

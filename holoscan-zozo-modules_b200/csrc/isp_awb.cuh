@@ -178,6 +178,12 @@ __device__ __forceinline__ void awb_tile_fmt(const FrameDesc& p, const uint8_t* 
 // `tiles_total` statistics tiles: block sums and bins into the frame's
 // scratch; the CTA that completes the count forms the frame's estimate
 // (awb_finish). The block's bins are left for the caller to clear.
+// With kAfterPrevious, the last CTA first waits (griddepcontrol.wait) for the
+// kernel this pass was launched behind: the single-frame pass may begin
+// while the previous frame's tile pass finishes, and only the estimate
+// (which reads and writes the white balance state that tile pass read) must
+// follow it.
+template <bool kAfterPrevious = false>
 __device__ void awb_flush(const FrameDesc& p, const u64 (&acc)[4], const unsigned int* hist, bool white_patch,
                           u64* red, int* first, bool* last, unsigned int tiles_done, unsigned int tiles_total) {
   Scratch* s = p.scratch;
@@ -198,6 +204,7 @@ __device__ void awb_flush(const FrameDesc& p, const u64 (&acc)[4], const unsigne
   if (tid == 0) *last = atomicAdd(&s->awb_done, tiles_done) + tiles_done == tiles_total;
   __syncthreads();
   if (*last) {
+    if constexpr (kAfterPrevious) griddep_wait();
     __threadfence();
     awb_finish(p, s, red, first);
   }

@@ -258,7 +258,7 @@ cudaError_t blocks_per_sm(LaunchShapes& shapes, const void* kernel, size_t smem_
 }
 
 cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes& shapes, cudaStream_t stream,
-                         cudaEvent_t before_main, cudaEvent_t after_main, const char** step) {
+                         cudaEvent_t before_main, cudaEvent_t after_main, const char** step, bool after_previous) {
   *step = "launch";
   const int threads = kernel_threads();
   const int pattern = d.pattern;
@@ -278,7 +278,24 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
     FrameDesc desc = d;
     void* args[] = {&map, &desc, &strips, &tiles_y, &band_tiles, &use_tma};
     *step = "white balance kernel launch";
-    const cudaError_t e2 = cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, smem, stream);
+    // With after_previous, as a programmatic dependent of the kernel queued
+    // just before it (the previous frame's tile pass, when frames follow each
+    // other on one stream): its CTAs sum this frame's raw samples on the SMs
+    // that pass leaves as it finishes, and its estimate waits in the kernel
+    // for that pass to complete. A kernel that does not signal its dependents
+    // early (griddepcontrol.launch_dependents) is waited for in full, as is
+    // any copy, event or other operation queued in between.
+    cudaLaunchConfig_t acfg{};
+    acfg.gridDim = dim3(blocks);
+    acfg.blockDim = dim3(threads);
+    acfg.dynamicSmemBytes = smem;
+    acfg.stream = stream;
+    cudaLaunchAttribute aattr[1];
+    aattr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    aattr[0].val.programmaticStreamSerializationAllowed = 1;
+    acfg.attrs = aattr;
+    acfg.numAttrs = after_previous ? 1 : 0;
+    const cudaError_t e2 = cudaLaunchKernelExC(&acfg, k, args);
     if (e2 != cudaSuccess) return e2;
   }
   const bool malvar = p.demosaic == ISP_DEMOSAIC_MALVAR;
@@ -450,19 +467,31 @@ int isp_b200_process(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp
   const FrameDesc d = make_desc(pl->params.c, pl->state, *raw, *out, stats, exposure);
   // Clear an error an earlier, unrelated call left (cuda_pipeline.cu:301-303).
   static_cast<void>(cudaGetLastError());
-  // Frames share the scratch and white balance state: on another stream,
-  // the GPU waits for the previous frame first (cuda_pipeline.cu:304-310).
+  // Frames share the scratch and white balance state: the GPU waits for the
+  // previous frame first (cuda_pipeline.cu:304-310). On the same stream the
+  // next frame's statistics pass may still overlap this one's end
+  // (frame_overlap): it follows the tile pass as its programmatic dependent.
+  const bool same_stream = pl->queued && stream == pl->last_stream;
   if (pl->queued) {
     error = cudaStreamWaitEvent(stream, pl->done, 0);
     if (error != cudaSuccess) return fail_cuda(error, "cudaStreamWaitEvent");
   }
   const char* step = "launch";
-  error = launch_frame(d, pl->params.c, shapes, stream, pl->before_main, pl->after_main, &step);
+  error = launch_frame(d, pl->params.c, shapes, stream, pl->before_main, pl->after_main, &step,
+                       same_stream && pl->frame_overlap);
   if (error == cudaSuccess) error = cudaGetLastError();
   if (error != cudaSuccess) return fail_cuda(error, (std::string("IspPipeline (cuda) ") + step).c_str());
   error = cudaEventRecord(pl->done, stream);
   if (error != cudaSuccess) return fail_cuda(error, "cudaEventRecord");
   pl->queued = true;
+  pl->last_stream = stream;
+  clear_error();
+  return ISP_OK;
+}
+
+int isp_b200_set_frame_overlap(isp_b200_pipeline* pl, int32_t enable) {
+  if (pl == nullptr) return fail(ISP_EINVAL, "pipeline is null");
+  pl->frame_overlap = enable != 0;
   clear_error();
   return ISP_OK;
 }
@@ -501,6 +530,7 @@ int isp_b200_check_bounded_wait(isp_b200_pipeline* pl, uint32_t polls, void* str
   if (error == cudaSuccess) error = cudaEventRecord(pl->done, stream);
   if (error != cudaSuccess) return fail_cuda(error, "isp_b200_check_bounded_wait");
   pl->queued = true;
+  pl->last_stream = stream;
   clear_error();
   return ISP_OK;
 }

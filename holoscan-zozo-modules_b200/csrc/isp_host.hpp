@@ -25,6 +25,9 @@ float white_level_of(const isp_params_c& p, int bit_depth);
 std::string validate_raw(const isp_raw_view_c& raw, const isp_params_c& p);
 std::string validate_out(const isp_raw_view_c& raw, const isp_rgb_view_c& out);
 std::vector<float> tone_lut(const isp_params_c& p);
+// tone_lut into `out` (room for the user table's size, or ISP_TONE_LUT_SIZE);
+// returns the entry count. Allocates nothing.
+size_t tone_table(const isp_params_c& p, float* out);
 
 // Thread-local error reporting behind isp_b200_last_error().
 int fail(int status, const std::string& message);
@@ -94,7 +97,7 @@ LaunchShapes& shapes_for_current_device(cudaError_t* error);
 // before_main / after_main (may be null) are recorded around the fused tile kernel.
 // `step` names the call that failed.
 cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes& shapes, cudaStream_t stream,
-                         cudaEvent_t before_main, cudaEvent_t after_main, const char** step);
+                         cudaEvent_t before_main, cudaEvent_t after_main, const char** step, bool after_previous = false);
 
 }  // namespace isp_b200
 
@@ -105,6 +108,8 @@ struct isp_b200_pipeline {
   int device = 0;
   cudaEvent_t done = nullptr;
   bool queued = false;
+  cudaStream_t last_stream = nullptr;  // the stream of the last queued frame
+  bool frame_overlap = true;           // isp_b200_set_frame_overlap
   // Staging for isp_b200_process_host, grown on demand.
   cudaStream_t host_stream = nullptr;
   void* d_raw = nullptr;

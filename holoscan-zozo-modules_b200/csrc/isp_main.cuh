@@ -373,6 +373,11 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
   // setup_frame reads) are visible. Without a programmatic launch it returns
   // at once.
   griddep_wait();
+  // The next frame's statistics pass may launch now (when queued right
+  // behind this kernel): it sums its own raw frame on the SMs this pass
+  // leaves as it finishes, and waits for this pass's completion before its
+  // estimate touches the white balance state read below.
+  griddep_launch_dependents();
   const FrameSetup f = setup_frame<kLutSmem, false>(p, m);
   __syncthreads();
 

@@ -66,6 +66,31 @@ def test_two_streams_in_call_order():
         _check("two_streams", f, frame.result(), case.expected[f], True)
 
 
+@pytest.mark.parametrize("overlap", [True, False])
+@pytest.mark.parametrize("name", ["sequence_two_streams", "awb_smoothing", "malvar_gray_world", "white_patch_sharp_rgba"])
+def test_frames_back_to_back_on_one_stream(name, overlap):
+    """Frames of one camera queued on one stream with nothing in between: each
+    frame's statistics pass may overlap the previous frame's tile pass (frame
+    overlap on) or follow it (off); either way every frame, white balance
+    smoothing included, is the reference's."""
+    torch = torch_cuda()
+    case = load_case(name)
+    stream = torch.cuda.Stream()
+    pipe = isp_b200.Pipeline(case.params)
+    pipe.set_frame_overlap(overlap)
+    frames = [DeviceFrame(raw, case.out_format, case.with_stats) for raw in case.frame_raws()]
+    torch.cuda.synchronize()
+    for frame in frames:
+        frame.run(pipe, case.exposure, stream.cuda_stream)
+    torch.cuda.synchronize()
+    for f, frame in enumerate(frames):
+        _check(name, f, frame.result(), case.expected[f], case.with_stats)
+    gains, valid = pipe.awb()
+    assert np.array_equal(np.array([*gains.view(np.uint32), valid], np.uint32), case.expected[-1]["awb"])
+    assert pipe.device_status() == 0
+    pipe.close()
+
+
 def test_determinism_and_fresh_instances():
     """determinism (pipeline_test.cpp:621-634)."""
     case = load_case("malvar_sharpened")
@@ -141,18 +166,6 @@ def test_full_size_configs_match_oracle(full_size_frames, which):
         assert same_bits(got.image, exp.image), f"{which} frame {f}: {first_mismatch(got.image, exp.image)}"
         assert np.array_equal(got.histogram, exp.histogram)
         assert same_bits(got.stats, exp.stats), f"{got.stats} vs {exp.stats}"
-
-
-def test_config2_8k_raw12_matches_oracle():
-    w = scene.config2()
-    raw = w.raw(11)
-    pipe = isp_b200.Pipeline(w.params)
-    ref = oracle.OraclePipeline(w.params)
-    got = run_device(pipe, raw, w.out_format, True, (20_000_000, 1.5))
-    exp = ref.process(raw, w.out_format, True, (20_000_000, 1.5))
-    assert same_bits(got.image, exp.image), first_mismatch(got.image, exp.image)
-    assert np.array_equal(got.histogram, exp.histogram)
-    assert same_bits(got.stats, exp.stats)
 
 
 def test_a_bounded_wait_that_runs_out_is_reported_and_the_next_frame_is_clean():
