@@ -12,16 +12,23 @@
 //
 // Host code cannot use that array's name as a device address (it is a host
 // stand-in); the first call on each device, with that device current, takes
-// the real address with cudaGetSymbolAddress and keeps it. That first call
-// should therefore come before any stream capture. Every call writes its
-// tables and clears its sums in the array on the caller's stream before its
-// kernels, so consecutive calls on one stream are ordered and each sees only
-// its own frame; calls that may overlap on the GPU (other streams, other
-// threads) race on the shared array and must not be issued.
+// the real address with cudaGetSymbolAddress, sets the kernels' shared-memory
+// limits and keeps both for that device's context (a device reset makes a new
+// context, and the next call sets up again). That first call should therefore
+// come before any stream capture. Every call stages its tables from host
+// memory that the next call reuses, so while its stream is capturing it
+// refuses (ISP_EINVAL) and queues nothing. Every call writes its tables and
+// clears its sums in the array on the caller's stream before its kernels, so
+// consecutive calls on one stream are ordered and each sees only its own
+// frame; calls that may overlap on the GPU (other streams, other threads)
+// race on the shared array and must not be issued.
 //
 // The frame is processed as the first frame of a fresh pipeline: an auto
 // white balance takes the frame's own estimate, unsmoothed. No cudaMalloc,
 // cudaFree or other allocating routine is called, on the device or the host.
+// isp_b200_noalloc_status reads (and clears) the array's flag that a bounded
+// wait gave up, after the stream's work is done and before the next call,
+// which clears it.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -52,8 +59,15 @@ static __device__ __align__(256) unsigned char g_noalloc[kNoAllocBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
-unsigned char* g_address[kMaxDevices] = {};
-int g_sm_count[kMaxDevices] = {};
+// Per device: the array's address in the context it was looked up in, that
+// context's id (a device reset makes a new context, and the lookup is
+// redone) and the SM count; the kernels' shared-memory limits are set then.
+struct DeviceSetup {
+  unsigned long long context = 0;
+  unsigned char* address = nullptr;
+  int sm_count = 0;
+};
+DeviceSetup g_setup[kMaxDevices];
 
 // Host-side staging of the tables (no heap): filled under g_mutex, copied to
 // the device before the lock is released (a copy from pageable memory
@@ -61,42 +75,66 @@ int g_sm_count[kMaxDevices] = {};
 float g_lut[kMaxToneEntries];
 float2 g_pairs[kMaxToneEntries];
 
-// The array's device address on the current device (set up on first use).
-cudaError_t noalloc_address(unsigned char** out, int* sm_count) {
+using CtxGetCurrent = CUresult (*)(CUcontext*);
+using CtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+
+void* driver_entry(const char* name) {
+  void* f = nullptr;
+  cudaDriverEntryPointQueryResult q{};
+  if (cudaGetDriverEntryPoint(name, &f, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess) {
+    return nullptr;
+  }
+  return f;
+}
+
+// The id of the context current on this thread, 0 when there is none yet.
+unsigned long long current_context_id() {
+  static const auto get_current = reinterpret_cast<CtxGetCurrent>(driver_entry("cuCtxGetCurrent"));
+  static const auto get_id = reinterpret_cast<CtxGetId>(driver_entry("cuCtxGetId"));
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current == nullptr || get_id == nullptr || get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr ||
+      get_id(ctx, &id) != CUDA_SUCCESS) {
+    return 0;
+  }
+  return id;
+}
+
+// Set-up on the current device: the array's device address (in host code its
+// name is only a stand-in), the SM count and every kernel's shared-memory
+// limit. Redone when the device's context changed since (after a reset).
+cudaError_t noalloc_setup(DeviceSetup** out) {
   int device = 0;
   cudaError_t e = cudaGetDevice(&device);
   if (e != cudaSuccess) return e;
   if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-  if (g_address[device] == nullptr) {
+  DeviceSetup& d = g_setup[device];
+  const unsigned long long ctx = current_context_id();
+  if (d.address == nullptr || ctx == 0 || ctx != d.context) {
     void* address = nullptr;
     e = cudaGetSymbolAddress(&address, g_noalloc);
     if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&g_sm_count[device], cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) return e;
-    g_address[device] = static_cast<unsigned char*>(address);
-  }
-  *out = g_address[device];
-  *sm_count = g_sm_count[device];
-  return cudaSuccess;
-}
-
-// tone_lut (isp_params.cpp:166-182) into g_lut; returns the entry count.
-size_t fill_tone(const isp_params_c& p) {
-  if (p.tone_curve == ISP_TONE_LUT) {
-    std::memcpy(g_lut, p.lut, p.lut_size * sizeof(float));
-    return p.lut_size;
-  }
-  for (int i = 0; i < ISP_TONE_LUT_SIZE; ++i) {
-    const double x = static_cast<double>(i) / (ISP_TONE_LUT_SIZE - 1);
-    double y = x;
-    if (p.tone_curve == ISP_TONE_SRGB) {
-      y = x <= 0.0031308 ? 12.92 * x : 1.055 * std::pow(x, 1.0 / 2.4) - 0.055;
-    } else if (p.tone_curve == ISP_TONE_GAMMA) {
-      y = std::pow(x, 1.0 / static_cast<double>(p.gamma));
+    e = cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, device);
+    for (int wp = 0; wp < 2 && e == cudaSuccess; ++wp) {
+      for (int pattern = 0; pattern < 4 && e == cudaSuccess; ++pattern) {
+        e = cudaFuncSetAttribute(awb_kernel(wp != 0, pattern), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(awb_kernel_smem()));
+      }
     }
-    g_lut[i] = static_cast<float>(y < 0.0 ? 0.0 : y > 1.0 ? 1.0 : y);
+    for (int k = 0; k < 64 && e == cudaSuccess; ++k) {
+      const bool malvar = (k & 1) != 0, sharpen = (k & 2) != 0, lut = (k & 8) != 0;
+      const int pattern = (k & 4) != 0 ? 2 : 0;
+      const int fmt = k >> 4;
+      const size_t most = main_kernel_smem(sharpen, kRawU16, lut ? kLutSmemEntries : 0);
+      e = cudaFuncSetAttribute(main_kernel(malvar, sharpen, pattern, lut, fmt),
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(most));
+    }
+    if (e != cudaSuccess) return e;
+    d.address = static_cast<unsigned char*>(address);
+    d.context = current_context_id();
   }
-  return ISP_TONE_LUT_SIZE;
+  *out = &d;
+  return cudaSuccess;
 }
 
 cudaError_t launch_noalloc(const FrameDesc& d, const isp_params_c& p, int sm_count, cudaStream_t stream) {
@@ -106,8 +144,7 @@ cudaError_t launch_noalloc(const FrameDesc& d, const isp_params_c& p, int sm_cou
     const void* k = awb_kernel(white_patch, d.pattern);
     const size_t smem = awb_kernel_smem();
     int bpsm = 0;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k, threads, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k, threads, smem);
     if (e != cudaSuccess) return e;
     alignas(64) CUtensorMap map;
     int use_tma = encode_raw_map(d, awb_box_row_bytes(d.raw_format), 64, &map) ? 1 : 0;
@@ -124,10 +161,8 @@ cudaError_t launch_noalloc(const FrameDesc& d, const isp_params_c& p, int sm_cou
   int lut_in_smem = d.tone_size <= kLutSmemEntries && with_lut <= kSmemPerTwoCtas ? 1 : 0;
   const size_t need = lut_in_smem ? with_lut : main_kernel_smem(sharpen, d.raw_format, 0);
   const void* k = main_kernel(p.demosaic == ISP_DEMOSAIC_MALVAR, sharpen, d.pattern, lut_in_smem != 0, d.out_format);
-  const size_t most = main_kernel_smem(sharpen, kRawU16, lut_in_smem ? kLutSmemEntries : 0);
   int bpsm = 0;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(most));
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k, threads, need);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k, threads, need);
   if (e != cudaSuccess) return e;
   alignas(64) CUtensorMap map;
   int use_tma = encode_raw_map(d, main_box_row_bytes(d.raw_format), main_box_rows(sharpen), &map) ? 1 : 0;
@@ -159,13 +194,23 @@ extern "C" int isp_b200_process_noalloc(const isp_params_c* params, const isp_ra
   if (const std::string why = validate_raw(*raw, *params); !why.empty()) return fail(ISP_EINVAL, why);
   if (const std::string why = validate_out(*raw, *out); !why.empty()) return fail(ISP_EINVAL, why);
   auto stream = static_cast<cudaStream_t>(stream_ptr);
+  // Every call stages its tables from host memory that the next call reuses:
+  // a stream capture would record copies of memory that changes under it.
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(stream, &capturing);
+  if (e != cudaSuccess) return fail_cuda(e, "isp_b200_process_noalloc: cudaStreamIsCapturing");
+  if (capturing != cudaStreamCaptureStatusNone) {
+    return fail(ISP_EINVAL, "isp_b200_process_noalloc: the stream is capturing; the call stages its tables from host "
+                            "memory that the next call reuses, so it queues nothing while capturing");
+  }
   std::lock_guard<std::mutex> lock(g_mutex);
-  unsigned char* base = nullptr;
-  int sm_count = 0;
-  cudaError_t e = noalloc_address(&base, &sm_count);
-  if (e != cudaSuccess) return fail_cuda(e, "isp_b200_process_noalloc: cudaGetSymbolAddress");
+  DeviceSetup* setup = nullptr;
+  e = noalloc_setup(&setup);
+  if (e != cudaSuccess) return fail_cuda(e, "isp_b200_process_noalloc: set-up");
+  unsigned char* base = setup->address;
+  const int sm_count = setup->sm_count;
   // The tables, as isp_b200_create keeps them (isp_capi.cu device_state_create).
-  const size_t n = fill_tone(*params);
+  const size_t n = tone_table(*params, g_lut);
   for (size_t i = 0; i + 1 < n; ++i) g_pairs[i] = make_float2(g_lut[i], g_lut[i + 1] - g_lut[i]);
   g_pairs[n - 1] = make_float2(g_lut[n - 1], 0.0F);
   DeviceState state;
@@ -194,6 +239,25 @@ extern "C" int isp_b200_process_noalloc(const isp_params_c* params, const isp_ra
   e = launch_noalloc(d, *params, sm_count, stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return fail_cuda(e, "isp_b200_process_noalloc");
+  clear_error();
+  return ISP_OK;
+}
+
+extern "C" int isp_b200_noalloc_status(void* stream_ptr, int32_t* status) {
+  if (status == nullptr) return fail(ISP_EINVAL, "status is null");
+  auto stream = static_cast<cudaStream_t>(stream_ptr);
+  std::lock_guard<std::mutex> lock(g_mutex);
+  DeviceSetup* setup = nullptr;
+  cudaError_t e = noalloc_setup(&setup);
+  if (e != cudaSuccess) return fail_cuda(e, "isp_b200_noalloc_status: set-up");
+  int* error = &reinterpret_cast<Scratch*>(setup->address + kScratchOffset)->error;
+  int value = 0;
+  const int zero = 0;
+  e = cudaStreamSynchronize(stream);
+  if (e == cudaSuccess) e = cudaMemcpy(&value, error, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(error, &zero, sizeof(int), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail_cuda(e, "isp_b200_noalloc_status");
+  *status = value;
   clear_error();
   return ISP_OK;
 }

@@ -162,11 +162,13 @@ std::string validate_out(const isp_raw_view_c& raw, const isp_rgb_view_c& out) {
   return {};
 }
 
-std::vector<float> tone_lut(const isp_params_c& p) {
+size_t tone_table(const isp_params_c& p, float* out) {
   // isp_params.cpp:166-182: the user's table verbatim, else 4097 points of
   // the curve evaluated in double and rounded to float.
-  if (p.tone_curve == ISP_TONE_LUT) return std::vector<float>(p.lut, p.lut + p.lut_size);
-  std::vector<float> lut(ISP_TONE_LUT_SIZE);
+  if (p.tone_curve == ISP_TONE_LUT) {
+    for (size_t i = 0; i < p.lut_size; ++i) out[i] = p.lut[i];
+    return p.lut_size;
+  }
   for (int i = 0; i < ISP_TONE_LUT_SIZE; ++i) {
     const double x = static_cast<double>(i) / (ISP_TONE_LUT_SIZE - 1);
     double y = x;
@@ -175,8 +177,14 @@ std::vector<float> tone_lut(const isp_params_c& p) {
     } else if (p.tone_curve == ISP_TONE_GAMMA) {
       y = std::pow(x, 1.0 / static_cast<double>(p.gamma));
     }
-    lut[static_cast<size_t>(i)] = static_cast<float>(y < 0.0 ? 0.0 : y > 1.0 ? 1.0 : y);
+    out[i] = static_cast<float>(y < 0.0 ? 0.0 : y > 1.0 ? 1.0 : y);
   }
+  return ISP_TONE_LUT_SIZE;
+}
+
+std::vector<float> tone_lut(const isp_params_c& p) {
+  std::vector<float> lut(p.tone_curve == ISP_TONE_LUT ? p.lut_size : size_t{ISP_TONE_LUT_SIZE});
+  tone_table(p, lut.data());
   return lut;
 }
 

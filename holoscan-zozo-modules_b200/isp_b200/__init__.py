@@ -68,9 +68,11 @@ def lib() -> C.CDLL:
                                        P(abi.ExposureC), C.c_void_p]
         L.isp_b200_process_noalloc.argtypes = [P(abi.ParamsC), P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
                                                P(abi.ExposureC), C.c_void_p]
+        L.isp_b200_noalloc_status.argtypes = [C.c_void_p, P(C.c_int32)]
         L.isp_b200_device_status.argtypes = [C.c_void_p, P(C.c_int32)]
         L.isp_b200_set_kernel_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.isp_b200_check_bounded_wait.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        L.isp_b200_set_frame_overlap.argtypes = [C.c_void_p, C.c_int32]
         L.isp_b200_process_host.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
                                             P(abi.ExposureC)]
         L.isp_b200_batch_create.argtypes = [C.c_int32, P(C.c_void_p)]
@@ -195,6 +197,11 @@ class Pipeline:
         v = C.c_int32()
         check(lib().isp_b200_device_status(self.handle, C.byref(v)))
         return int(v.value)
+
+    def set_frame_overlap(self, enable: bool) -> None:
+        """On (default): a frame queued right behind the previous one on the same stream starts its statistics
+        pass while that frame's tile pass finishes."""
+        check(lib().isp_b200_set_frame_overlap(self.handle, 1 if enable else 0))
 
     def check_bounded_wait(self, polls: int = 1024, stream: int = 0) -> None:
         """Queues a kernel whose bounded barrier wait runs out after `polls` polls and flags this camera
@@ -387,6 +394,14 @@ def process_noalloc(params: IspParams, raw: abi.RawViewC, out: abi.RgbViewC, his
     exp = abi.ExposureC(exposure[0], exposure[1])
     check(lib().isp_b200_process_noalloc(h.ref(), C.byref(raw), C.byref(out), C.byref(st), C.byref(exp),
                                          stream or None))
+
+
+def noalloc_status(stream: int = 0) -> int:
+    """After `stream`'s work: 1 if a kernel of the last no-alloc frame gave up a bounded wait, else 0
+    (isp_b200_noalloc_status; read and cleared, allocating nothing)."""
+    v = C.c_int32()
+    check(lib().isp_b200_noalloc_status(stream or None, C.byref(v)))
+    return int(v.value)
 
 
 def view_compose(raw: abi.RawViewC, black_level: float, rgb8_ptr: int, rgb8_pitch: int, view_ptr: int,

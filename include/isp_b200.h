@@ -399,13 +399,34 @@ ISP_B200_API int isp_b200_view_compose(const isp_raw_view_c* raw, float black_le
  * which every GPU that loads it holds until exit; larger tables are refused
  * with ISP_EINVAL. The frame is processed as the first frame of a fresh
  * pipeline (auto white balance: its own estimate, unsmoothed). The first call
- * on a device, with that device current, looks up the array's address; make
- * it before any stream capture. Calls share the array: consecutive calls on
- * one stream are ordered, calls that overlap on the GPU race. No cudaMalloc,
- * cudaFree or other allocating routine is called. */
+ * on a device, with that device current, looks up the array's address and
+ * sets the kernels' limits (again after a device reset); make it before any
+ * stream capture. Each call stages its tables from host memory that the next
+ * call reuses, so it returns ISP_EINVAL and queues nothing while `stream` is
+ * capturing. Calls share the array: consecutive calls on one stream are
+ * ordered, calls that overlap on the GPU race. No cudaMalloc, cudaFree or
+ * other allocating routine is called. */
 ISP_B200_API int isp_b200_process_noalloc(const isp_params_c* params, const isp_raw_view_c* raw,
                              const isp_rgb_view_c* out, const isp_stats_c* stats,
                              const isp_exposure_c* exposure, void* stream);
+
+/* Companion of isp_b200_process_noalloc, no reference counterpart, also
+ * allocating nothing: waits for `stream`, then reports (and clears) whether a
+ * kernel of the last no-alloc frame on the current device gave up a bounded
+ * wait (*status 1: that frame's outputs are not trustworthy), else 0. Call it
+ * before the next no-alloc call, which clears the flag. */
+ISP_B200_API int isp_b200_noalloc_status(void* stream, int32_t* status);
+
+/* Frame overlap, no reference counterpart (on by default): when frames of
+ * one pipeline follow each other on one stream, the next frame's white
+ * balance statistics pass may begin while the previous frame's tile pass
+ * finishes (a programmatic dependent launch); its estimate still waits for
+ * that pass, so every output is the one the frames give alone. The pass reads
+ * its raw frame before that wait, so a kernel queued just before the call
+ * that writes the raw frame must not signal its dependents early
+ * (griddepcontrol.launch_dependents / cudaTriggerProgrammaticLaunchCompletion);
+ * ordinary kernels, copies and events are waited for in full. 0 turns it off. */
+ISP_B200_API int isp_b200_set_frame_overlap(isp_b200_pipeline* pipeline, int32_t enable);
 
 /* Device-side status, no reference counterpart: waits for the pipeline's
  * queued frames, then reports (and clears) whether a kernel gave up a bounded
