@@ -20,6 +20,13 @@ the device->host copy of the image, histogram and statistics, every step).
 event-timed duration. `cpu_baseline` is the reference's CPU backend (built
 from its sources into oracle/_ref) on the host cores, a bounded sample.
 
+At one GPU the default c1 line also carries `batch` (c3: the 48-camera
+mixed batch as one replayed graph per step against the same frames through
+the per-frame path) and `serving` (c4, bounded: the 64 streams at their
+nominal Poisson rates for the latency percentiles, then saturation runs
+batched and per frame), so that both are measured on the same box under the
+same clock; --no-extras leaves them out.
+
 --impl reference times that CPU backend alone on the same workload and prints
 the same line with "impl": "reference".
 
@@ -66,6 +73,9 @@ def parse_args():
     ap.add_argument("--aux-seconds", type=float, default=15.0, help="c4: the other serving runs")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="c1 at one GPU: skip the batch and serving keys")
+    ap.add_argument("--serving-seconds", type=float, default=20.0, help="c1's serving key: the nominal-rate run")
+    ap.add_argument("--serving-sat-seconds", type=float, default=5.0, help="c1's serving key: each saturation run")
     ap.add_argument("--no-cases", action="store_true", help="convert: the headline case only")
     ap.add_argument("--fresh-frames", type=int, default=0,
                     help="c2: render this many fresh-seed frames instead of the workload's 200 (small profiling runs)")
@@ -298,6 +308,46 @@ def rotating_sets(w: scene.Workload) -> int:
 
 # ---- GPU ---------------------------------------------------------------------
 
+def batch_summary(steps: int, warmup: int, barrier, clocks=None) -> dict:
+    """c3 at one GPU for the default line's `batch` key: the 48-frame mixed
+    batch replayed as a CUDA graph against the same frames through the
+    per-frame path, device-resident inputs, CUDA-event timed."""
+    core = batch_core(steps, warmup, 0, barrier, clocks)
+    info = core["batch"].info()
+    core["batch"].close()
+    per_step = core["elapsed_ms"] / steps
+    px = core["total_px"]
+    return {"workload": "c3_mixed_batch_48_frames", "value": px / (per_step / 1e3) / 1e9, "unit": "Gpix/s",
+            "ms_per_step": per_step, "steps": steps, "warmup": warmup, "pixels_per_step": px,
+            "per_frame_path_value": px / (core["plain_ms"] / 1e3) / 1e9, "per_frame_path_ms_per_step": core["plain_ms"],
+            "batched_over_per_frame": core["plain_ms"] / per_step,
+            "launch": "descriptor staging + statistics pass + tile pass per step, replayed CUDA graph; per-frame "
+                      "path: one isp_b200_process per frame on one stream",
+            "autotune": info, "clocks": core["clocks"]}
+
+
+def serving_summary(nominal_seconds: float, sat_seconds: float, barrier, clocks=None) -> dict:
+    """c4 at one GPU for the default line's `serving` key, bounded: the 64
+    streams at their nominal Poisson rates with host-memory arrivals for
+    `nominal_seconds` (latency percentiles), then closed-loop saturation runs
+    of `sat_seconds`, batched and per frame, with device-memory arrivals."""
+    cams, fps, budget, serve, brief = serving_setup(0, barrier)
+    nominal = serve(False, False, False, nominal_seconds, clocks)
+    sat = serve(False, True, True, sat_seconds)
+    sat_plain = serve(True, True, True, sat_seconds)
+    ratio = sat["gpix_per_s"] / max(1e-9, sat_plain["gpix_per_s"])
+    return {"workload": "c4_serving_64_streams", "unit": "Gpix/s",
+            "latency_ms": {"p50": nominal["p50_ms"], "p99": nominal["p99_ms"], "p99.9": nominal["p999_ms"],
+                           "max": nominal["max_ms"], "arrivals": "host memory (copied in), nominal rate",
+                           "seconds": nominal_seconds},
+            "nominal": brief(nominal), "offered_gpix_s": sum(c.pixels * f for c, f in zip(cams, fps)) / 1e9,
+            "saturation_value": sat["gpix_per_s"], "saturation": brief(sat),
+            "per_frame_path_value": sat_plain["gpix_per_s"], "per_frame_path": brief(sat_plain),
+            "batched_over_per_frame": ratio, "saturation_seconds": sat_seconds, "memory_budget_bytes": budget,
+            "targets": {"batched_at_least_2x_per_frame": ratio >= 2.0, "p99_at_most_1_ms": nominal["p99_ms"] <= 1.0},
+            "clocks": nominal["clocks"]}
+
+
 def run_b200(args):
     import torch
 
@@ -527,6 +577,13 @@ def run_b200(args):
     if dist is not None:
         dist.barrier()
     pipe.close()
+
+    # c3 and c4 beside c1 at one GPU (the default run): the batched launch
+    # and the serving loop on the same box, under the same clock.
+    extras = {}
+    if world == 1 and args.workload == "c1" and not args.no_extras:
+        extras["batch"] = batch_summary(max(20, min(args.steps, 200)), max(3, args.warmup), barrier, Clocks(local))
+        extras["serving"] = serving_summary(args.serving_seconds, args.serving_sat_seconds, barrier, Clocks(local))
     if rank == 0:
         peak, peak_kind = measured_peak()
         achieved = w.compulsory_bytes() / (kernel_ms / 1e3) / 1e9
@@ -548,10 +605,72 @@ def run_b200(args):
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clock_info,
             "reference_gpu": ref_gpu,
+            **extras,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def batch_core(steps: int, warmup: int, rank: int, barrier, clocks=None) -> dict:
+    """c3's timed core: the 48 cameras' device-rendered frames through the
+    batch (autotuned, replayed CUDA graph) for `steps` launches after
+    `warmup`, then the same frames through the per-frame path (one
+    isp_b200_process each). Times are CUDA events on the launching stream."""
+    import torch
+
+    import isp_b200
+
+    cams = scene.mixed_cameras(seed=2024)
+    pipes = [isp_b200.Pipeline(c.params) for c in cams]
+    frames = []
+    for i, c in enumerate(cams):
+        data, row = device_frame(c, 7000 * (rank + 1) + i)
+        out_row = c.width * 3
+        out = torch.empty(c.height * out_row, dtype=torch.uint8, device="cuda")
+        hist = torch.empty(1024, dtype=torch.int32, device="cuda")
+        st = torch.empty(12, dtype=torch.float32, device="cuda")
+        rv = abi.RawViewC(data.data_ptr(), c.width, c.height, row, c.fmt, c.bits, c.pattern)
+        ov = abi.RgbViewC(out.data_ptr(), out_row, abi.RGB8)
+        frames.append((data, out, hist, st, rv, ov, row, out_row))
+    total_px = sum(c.pixels for c in cams)
+    batch = isp_b200.Batch(len(cams))
+    for pipe, (data, out, hist, st, rv, ov, row, out_row) in zip(pipes, frames):
+        batch.add(pipe, rv, ov, hist.data_ptr(), st.data_ptr(), (10_000_000, 1.5))
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    batch.autotune(sptr)
+    for _ in range(warmup):
+        batch.launch(sptr, True)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    if clocks is not None:
+        clocks.start()
+    time.sleep(0.3)
+    barrier()
+    start.record(stream)
+    for _ in range(steps):
+        batch.launch(sptr, True)
+    end.record(stream)
+    barrier()
+    clock_info = clocks.stop() if clocks is not None else None
+    elapsed_ms = start.elapsed_time(end)
+    # The same frames through the per-frame path (one isp_b200_process each).
+    for _ in range(2):
+        for pipe, (data, out, hist, st, rv, ov, row, out_row) in zip(pipes, frames):
+            pipe.process(rv, ov, hist.data_ptr(), st.data_ptr(), (10_000_000, 1.5), sptr)
+    p_start, p_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    plain_steps = max(3, steps // 2)
+    barrier()
+    p_start.record(stream)
+    for _ in range(plain_steps):
+        for pipe, (data, out, hist, st, rv, ov, row, out_row) in zip(pipes, frames):
+            pipe.process(rv, ov, hist.data_ptr(), st.data_ptr(), (10_000_000, 1.5), sptr)
+    p_end.record(stream)
+    barrier()
+    plain_ms = p_start.elapsed_time(p_end) / plain_steps
+    return {"cams": cams, "pipes": pipes, "frames": frames, "batch": batch, "stream": stream, "total_px": total_px,
+            "elapsed_ms": elapsed_ms, "plain_ms": plain_ms, "clocks": clock_info}
 
 
 def run_batch(args):
@@ -577,54 +696,10 @@ def run_batch(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    cams = scene.mixed_cameras(seed=2024)
-    pipes = [isp_b200.Pipeline(c.params) for c in cams]
-    frames = []
-    for i, c in enumerate(cams):
-        data, row = device_frame(c, 7000 * (rank + 1) + i)
-        out_row = c.width * 3
-        out = torch.empty(c.height * out_row, dtype=torch.uint8, device="cuda")
-        hist = torch.empty(1024, dtype=torch.int32, device="cuda")
-        st = torch.empty(12, dtype=torch.float32, device="cuda")
-        rv = abi.RawViewC(data.data_ptr(), c.width, c.height, row, c.fmt, c.bits, c.pattern)
-        ov = abi.RgbViewC(out.data_ptr(), out_row, abi.RGB8)
-        frames.append((data, out, hist, st, rv, ov, row, out_row))
-    total_px = sum(c.pixels for c in cams)
-    batch = isp_b200.Batch(len(cams))
-    for pipe, (data, out, hist, st, rv, ov, row, out_row) in zip(pipes, frames):
-        batch.add(pipe, rv, ov, hist.data_ptr(), st.data_ptr(), (10_000_000, 1.5))
-    stream = torch.cuda.Stream()
+    core = batch_core(args.steps, args.warmup, rank, barrier, Clocks(local))
+    cams, pipes, frames, batch, stream = core["cams"], core["pipes"], core["frames"], core["batch"], core["stream"]
     sptr = stream.cuda_stream
-    batch.autotune(sptr)
-    for _ in range(args.warmup):
-        batch.launch(sptr, True)
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    clocks = Clocks(local)
-    clocks.start()
-    time.sleep(0.3)
-    barrier()
-    start.record(stream)
-    for _ in range(args.steps):
-        batch.launch(sptr, True)
-    end.record(stream)
-    barrier()
-    clock_info = clocks.stop()
-    elapsed_ms = start.elapsed_time(end)
-    # The same frames through the per-frame path (one isp_b200_process each).
-    for _ in range(2):
-        for pipe, (data, out, hist, st, rv, ov, row, out_row) in zip(pipes, frames):
-            pipe.process(rv, ov, hist.data_ptr(), st.data_ptr(), (10_000_000, 1.5), sptr)
-    p_start, p_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    plain_steps = max(3, args.steps // 2)
-    barrier()
-    p_start.record(stream)
-    for _ in range(plain_steps):
-        for pipe, (data, out, hist, st, rv, ov, row, out_row) in zip(pipes, frames):
-            pipe.process(rv, ov, hist.data_ptr(), st.data_ptr(), (10_000_000, 1.5), sptr)
-    p_end.record(stream)
-    barrier()
-    plain_ms = p_start.elapsed_time(p_end) / plain_steps
+    total_px, elapsed_ms, plain_ms, clock_info = core["total_px"], core["elapsed_ms"], core["plain_ms"], core["clocks"]
     elapsed_max = max_over_ranks(elapsed_ms, dist)
     value = whole_job_rate(args.steps * total_px, elapsed_ms / 1e3, world, dist) / 1e9
     # End to end: every step copies each frame's raw from pinned host memory,
@@ -767,34 +842,17 @@ def cpu_mixed_baseline(cams, picks, seconds: float):
                       f"for {secs:.1f} s"}
 
 
-def run_serving(args):
-    """Serving: 64 camera streams (four shapes, nominal 120/60/30/15 fps) with
-    seeded Poisson arrivals through the continuous-batching server, against
-    the same server launching each frame alone (the plain per-frame path).
-
-    Latency percentiles come from the nominal-rate runs: a frame's latency is
-    its arrival (host memory, copied to the device from pinned memory) to
-    the completion of its image, histogram and statistics in device memory,
-    seen by the server polling its batch's event. Throughput comes from
-    closed-loop runs at saturation (every stream's queue kept full):
-    completed pixels over first arrival to last completion. `value` is the
-    saturation throughput with frames arriving in device memory (as from a
-    capture device writing to HBM); `e2e` is the same with frames arriving in
-    host memory (copied to the device per frame) and every frame's image,
-    histogram and statistics copied back."""
+def serving_setup(rank: int, barrier):
+    """c4's 64 streams (three device-rendered fresh-seed frames each, held in
+    host memory) and a runner: serve(per_frame, on_device, closed, seconds,
+    clocks, copy_back) runs a server for one second of warm-up arrivals, then
+    `seconds` of seeded Poisson arrivals at the nominal rates (or a closed
+    loop at saturation), drains it and returns its statistics; brief(st)
+    keeps the reported fields."""
     import torch
 
     import isp_b200
 
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
     cams, fps = scene.serving_streams()
     n_sources = 3
     sources = []
@@ -818,11 +876,6 @@ def run_serving(args):
                 sv.add_source(sid, r, on_device)
         sv.start()
         return sv
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
 
     def serve(per_frame: bool, on_device: bool, closed: bool, seconds: float, clocks=None, copy_back=False):
         sv = make_server(per_frame, on_device, copy_back)
@@ -852,6 +905,45 @@ def run_serving(args):
     def brief(st):
         return {k: st[k] for k in ("gpix_per_s", "p50_ms", "p99_ms", "p999_ms", "max_ms", "p50_wait_ms",
                                    "p99_wait_ms", "completed", "refused", "batches", "mean_batch_frames")}
+
+    return cams, fps, budget, serve, brief
+
+
+def run_serving(args):
+    """Serving: 64 camera streams (four shapes, nominal 120/60/30/15 fps) with
+    seeded Poisson arrivals through the continuous-batching server, against
+    the same server launching each frame alone (the plain per-frame path).
+
+    Latency percentiles come from the nominal-rate runs: a frame's latency is
+    its arrival (host memory, copied to the device from pinned memory) to
+    the completion of its image, histogram and statistics in device memory,
+    seen by the server polling its batch's event. Throughput comes from
+    closed-loop runs at saturation (every stream's queue kept full):
+    completed pixels over first arrival to last completion. `value` is the
+    saturation throughput with frames arriving in device memory (as from a
+    capture device writing to HBM); `e2e` is the same with frames arriving in
+    host memory (copied to the device per frame) and every frame's image,
+    histogram and statistics copied back."""
+    import torch
+
+    import isp_b200
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    cams, fps, budget, serve, brief = serving_setup(rank, barrier)
 
     nominal_host = serve(False, False, False, args.seconds, Clocks(local))
     nominal_device = serve(False, True, False, args.aux_seconds)

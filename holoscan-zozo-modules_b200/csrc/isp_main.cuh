@@ -139,6 +139,38 @@ __device__ __forceinline__ void unit_rc(int u, bool same_parity, int& r, int& uc
   r = same_parity ? ((w >> 1) << 3) + 2 * ro + (w & 1) : 4 * w + ro;
 }
 
+// The per-pixel tail of four pairs of one output row (pixels x .. x + 3 and
+// x + 32 .. x + 35 of row y): colour matrix, statistics, tone, store and
+// histograms, with the per-pixel guards only where the row leaves the image
+// or the output rows are not 16-byte aligned. kOutSel: the output format
+// fixed at compile time (the single-frame kernels), or -1 to choose it per
+// unit (the batch kernel).
+template <int kOutSel, bool kLutSmem>
+__device__ __forceinline__ void finish_row(const FrameDesc& p, const FrameSetup& f, unsigned int* hist,
+                                           const float2 (&rgb)[4][3], int x, int y, unsigned int (&sums)[3],
+                                           unsigned int& npix) {
+  if (y >= p.height) return;
+  const int nl = min(max(p.width - x, 0), 4);
+  const int nr = min(max(p.width - x - kHalf, 0), 4);
+  if (nl == 4 && nr == 4 && p.out_vector) {
+    if constexpr (kOutSel < 0) {
+      finish_pairs_any<kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, hist, sums,
+                                       npix);
+    } else {
+      finish_pairs<kOutSel, kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, hist,
+                                            sums, npix);
+    }
+  } else {
+    if constexpr (kOutSel < 0) {
+      finish_pairs_any<kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, hist,
+                                        sums, npix);
+    } else {
+      finish_pairs<kOutSel, kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
+                                             hist, sums, npix);
+    }
+  }
+}
+
 // One 64x64 tile at (x0, y0). `map` is the frame's TMA descriptor (its box
 // is waited for on `bar`); after phase A, when the box is free again,
 // `after_a()` runs (to prefetch the next tile). Adds the tile's statistics
@@ -190,38 +222,11 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
     __syncthreads();
   }
 
-  // C. The per-pixel tail of four pairs of one row (x .. x + 3 and
-  //    x + 32 .. x + 35). The statistics sums stay below 2^32 per thread and
-  //    tile (16 pixels of at most 2^20).
+  // C. The statistics sums stay below 2^32 per thread and tile (16 pixels
+  //    of at most 2^20).
   unsigned int sums[3] = {0U, 0U, 0U};
   unsigned int npix = 0;
-  const auto finish_row = [&](const float2 (&rgb)[4][3], int r, int uc) {
-    const int x = x0 + 4 * uc;
-    const int y = y0 + r;
-    if (y >= p.height) return;
-    const int nl = min(max(p.width - x, 0), 4);
-    const int nr = min(max(p.width - x - kHalf, 0), 4);
-    // kOutSel: the output format fixed at compile time (the single-frame
-    // kernels), or -1 to choose it per unit (the batch kernel).
-    if (nl == 4 && nr == 4 && p.out_vector) {
-      if constexpr (kOutSel < 0) {
-        finish_pairs_any<kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist,
-                                         sums, npix);
-      } else {
-        finish_pairs<kOutSel, kLutSmem, true>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
-                                              m.hist, sums, npix);
-      }
-    } else {
-      if constexpr (kOutSel < 0) {
-        finish_pairs_any<kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist, m.hist,
-                                          sums, npix);
-      } else {
-        finish_pairs<kOutSel, kLutSmem, false>(p, rgb, x, y, nl, nr, f.lut, f.lut_scale, f.want_stats, f.want_hist,
-                                               m.hist, sums, npix);
-      }
-    }
-  };
-  if constexpr (kSharpen) {
+  if constexpr (kSharpen && kOutSel >= 0) {
     // One unit per thread: output rows r and r + 1 of group uc, whose RGB
     // rows r .. r + 3 each plane loads once.
     int r, uc;
@@ -247,29 +252,45 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
       rgb0[i][2] = o0[i];
       rgb1[i][2] = o1[i];
     }
-    finish_row(rgb0, r, uc);
-    finish_row(rgb1, r + 1, uc);
+    finish_row<kOutSel, kLutSmem>(p, f, m.hist, rgb0, x0 + 4 * uc, y0 + r, sums, npix);
+    finish_row<kOutSel, kLutSmem>(p, f, m.hist, rgb1, x0 + 4 * uc, y0 + r + 1, sums, npix);
   } else {
-    // Two units of four pairs of one row per thread, straight from the samples.
+    // Two units of four pairs of one row per thread: sharpened (the batch
+    // kernel, whose output format is chosen per unit, keeps one call site of
+    // the finish), or demosaiced straight from the samples.
 #pragma unroll 1
     for (int k = 0; k < 2; ++k) {
       int r, uc;
       unit_rc(tid + k * kThreads, true, r, uc);
       float2 rgb[4][3];
-      if (r & 1) {
-        demosaic_row4<kMalvar, kPat, 1>(m.P, r, uc, rgb);
-      } else {
-        demosaic_row4<kMalvar, kPat, 0>(m.P, r, uc, rgb);
-      }
-      if (f.swap_rb) {
+      if constexpr (kSharpen) {
+        const float2 amount = bc2(p.sharpen);
+        float2 o[4];
+        sharpen_row1(m.R, r, uc, amount, o);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float2 red = rgb[i][0];
-          rgb[i][0] = rgb[i][2];
-          rgb[i][2] = red;
+        for (int i = 0; i < 4; ++i) rgb[i][0] = o[i];
+        sharpen_row1(m.G, r, uc, amount, o);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) rgb[i][1] = o[i];
+        sharpen_row1(m.B, r, uc, amount, o);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) rgb[i][2] = o[i];
+      } else {
+        if (r & 1) {
+          demosaic_row4<kMalvar, kPat, 1>(m.P, r, uc, rgb);
+        } else {
+          demosaic_row4<kMalvar, kPat, 0>(m.P, r, uc, rgb);
+        }
+        if (f.swap_rb) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float2 red = rgb[i][0];
+            rgb[i][0] = rgb[i][2];
+            rgb[i][2] = red;
+          }
         }
       }
-      finish_row(rgb, r, uc);
+      finish_row<kOutSel, kLutSmem>(p, f, m.hist, rgb, x0 + 4 * uc, y0 + r, sums, npix);
     }
   }
 #pragma unroll

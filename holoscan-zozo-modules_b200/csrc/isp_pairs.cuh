@@ -248,6 +248,33 @@ __device__ __forceinline__ void sharpen_rows2(const float2* X, int r, int uc, fl
   }
 }
 
+// C (sharpening), one output row: the 3x3 windows of one plane around pairs
+// 4uc .. 4uc + 3 of output row r, sharpened from RGB rows r .. r + 2 (loaded
+// as in sharpen_rows2; a quarter-warp takes rows r and r + 2, which csw
+// sends to different banks).
+__device__ __forceinline__ void sharpen_row1(const float2* X, int r, int uc, float2 amount, float2 (&o)[4]) {
+  float2 w[3][6];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int j = r + a;
+    const int s = csw(j);
+    const float2* row = X + j * kCW2;
+    const float4 v0 = lds4(row + 2 * ((2 * uc) ^ s)), v1 = lds4(row + 2 * ((2 * uc + 1) ^ s)),
+                 v2 = lds4(row + 2 * cchunk(2 * uc + 2, s));
+    w[a][0] = lo2(v0);
+    w[a][1] = hi2(v0);
+    w[a][2] = lo2(v1);
+    w[a][3] = hi2(v1);
+    w[a][4] = lo2(v2);
+    w[a][5] = hi2(v2);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    o[i] = sharpen_one2(w[1][i + 1], w[0][i + 1], w[2][i + 1], w[1][i], w[1][i + 2], w[0][i], w[0][i + 2], w[2][i],
+                        w[2][i + 2], amount);
+  }
+}
+
 // C (no sharpening). Demosaic pairs 4uc .. 4uc + 3 of output row r straight
 // from the samples: sample rows r .. r + 4 (halo 2), pair columns 4uc + 2 ..
 // 4uc + 9. kRowPar: the parity of the output row.
