@@ -26,7 +26,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden",
           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-DISP_B200_BUILD"]
 
-SOURCES = ["isp_batch.cu", "isp_batch_global_lut.cu", "isp_main_bilinear.cu", "isp_main_bilinear_sharpen.cu", "isp_main_malvar.cu", "isp_main_malvar_sharpen.cu",
+SOURCES = ["isp_batch.cu", "isp_batch_global_lut.cu", "isp_batch_short.cu", "isp_batch_short_global_lut.cu",
+           "isp_main_bilinear.cu", "isp_main_bilinear_sharpen.cu", "isp_main_malvar.cu", "isp_main_malvar_sharpen.cu",
+           "isp_main_bilinear_short.cu", "isp_main_bilinear_sharpen_short.cu", "isp_main_malvar_short.cu",
+           "isp_main_malvar_sharpen_short.cu",
            "isp_awb.cu", "isp_kernels.cu", "isp_capi.cu", "isp_batch_host.cu", "isp_noalloc.cu", "isp_server.cu", "isp_synth.cu", "isp_view.cu", "isp_params.cpp",
            # the colour converter (the step after the ISP)
            "cc/cc_direct_yuv.cu", "cc/cc_direct_rgb.cu", "cc/cc_direct_gray.cu", "cc/cc_resample.cu", "cc/cc_capi.cu",

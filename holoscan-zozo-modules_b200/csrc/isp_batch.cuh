@@ -40,13 +40,14 @@ __device__ __forceinline__ int frame_of_item(const BatchFrame* frames, int nfram
   return f;
 }
 
-template <bool kLutSmem>
-__global__ void __launch_bounds__(kThreads, 2) isp_batch_kernel(const BatchFrame* frames, int nframes,
-                                                                const int2* ranges) {
-  using GS = Geom<true>;  // the sharpening geometry holds every variant's
+template <bool kLutSmem, int kTileH>
+__global__ void __launch_bounds__(kThreads, kTileH == kTH ? 2 : 3)
+    isp_batch_kernel(const BatchFrame* frames, int nframes, const int2* ranges) {
+  using GS = Geom<true, kTileH>;  // the sharpening geometry holds every variant's
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
-  const TileSmem m = carve(smem, layout_of(true, box_row_bytes(kRawU16), kLutSmem ? kBatchLutEntries : 0), GS::kSH);
+  const TileSmem m =
+      carve(smem, layout_of(true, box_row_bytes(kRawU16), kLutSmem ? kBatchLutEntries : 0, kTileH), GS::kSH);
   __shared__ uint64_t bar;
   __shared__ u64 red[4 * kWarps];
   __shared__ int minmax[2];
@@ -73,8 +74,8 @@ __global__ void __launch_bounds__(kThreads, 2) isp_batch_kernel(const BatchFrame
     const int halo = (bf.variant & 2) ? 4 : 2;
     const int fmt = bf.desc.raw_format;
     tensormap_acquire(&bf.main_map);
-    tma_load_2d(&bf.main_map, m.box, &bar, box_x(fmt, x0), ty * kTH - halo,
-                static_cast<unsigned int>((kTH + 2 * halo) * box_row_bytes(fmt)));
+    tma_load_2d(&bf.main_map, m.box, &bar, box_x(fmt, x0), ty * kTileH - halo,
+                static_cast<unsigned int>((kTileH + 2 * halo) * box_row_bytes(fmt)));
   };
   if (tid == 0 && frames[f].use_tma) issue(f, r.x);
   uint32_t phase = 0;
@@ -108,14 +109,14 @@ __global__ void __launch_bounds__(kThreads, 2) isp_batch_kernel(const BatchFrame
       }
     };
     switch (bf.variant) {
-      case 0: run_tile<false, false, 0, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
-      case 1: run_tile<true, false, 0, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
-      case 2: run_tile<false, true, 0, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
-      case 3: run_tile<true, true, 0, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
-      case 4: run_tile<false, false, 1, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
-      case 5: run_tile<true, false, 1, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
-      case 6: run_tile<false, true, 1, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
-      default: run_tile<true, true, 1, kLutSmem>(fd, fs, m, minmax, x0, ty * kTH, use_tma, &bar, phase, acc, prefetch); break;
+      case 0: run_tile<false, false, 0, kLutSmem, decltype(prefetch), -1, kTileH>(fd, fs, m, minmax, x0, ty * kTileH, use_tma, &bar, phase, acc, prefetch); break;
+      case 1: run_tile<true, false, 0, kLutSmem, decltype(prefetch), -1, kTileH>(fd, fs, m, minmax, x0, ty * kTileH, use_tma, &bar, phase, acc, prefetch); break;
+      case 2: run_tile<false, true, 0, kLutSmem, decltype(prefetch), -1, kTileH>(fd, fs, m, minmax, x0, ty * kTileH, use_tma, &bar, phase, acc, prefetch); break;
+      case 3: run_tile<true, true, 0, kLutSmem, decltype(prefetch), -1, kTileH>(fd, fs, m, minmax, x0, ty * kTileH, use_tma, &bar, phase, acc, prefetch); break;
+      case 4: run_tile<false, false, 1, kLutSmem, decltype(prefetch), -1, kTileH>(fd, fs, m, minmax, x0, ty * kTileH, use_tma, &bar, phase, acc, prefetch); break;
+      case 5: run_tile<true, false, 1, kLutSmem, decltype(prefetch), -1, kTileH>(fd, fs, m, minmax, x0, ty * kTileH, use_tma, &bar, phase, acc, prefetch); break;
+      case 6: run_tile<false, true, 1, kLutSmem, decltype(prefetch), -1, kTileH>(fd, fs, m, minmax, x0, ty * kTileH, use_tma, &bar, phase, acc, prefetch); break;
+      default: run_tile<true, true, 1, kLutSmem, decltype(prefetch), -1, kTileH>(fd, fs, m, minmax, x0, ty * kTileH, use_tma, &bar, phase, acc, prefetch); break;
     }
     ++done;
   }

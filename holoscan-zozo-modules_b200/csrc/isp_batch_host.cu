@@ -56,8 +56,10 @@ struct Shape {
   int main_ctas = 0;
   int awb_ctas = 0;
   bool lut_smem = false;
+  int tile_rows = 64;
   bool operator==(const Shape& o) const {
-    return nframes == o.nframes && main_ctas == o.main_ctas && awb_ctas == o.awb_ctas && lut_smem == o.lut_smem;
+    return nframes == o.nframes && main_ctas == o.main_ctas && awb_ctas == o.awb_ctas && lut_smem == o.lut_smem &&
+           tile_rows == o.tile_rows;
   }
 };
 
@@ -77,6 +79,7 @@ struct isp_b200_batch {
   int next_slot = 0;
   float weights[4] = {kDefaultWeights[0], kDefaultWeights[1], kDefaultWeights[2], kDefaultWeights[3]};
   int ctas_per_sm = 0;  // 0: as many as fit
+  int tile_rows = 64;   // the tile pass's tile height: 64 or 32
   bool tuned = false;
   // The graph of the last shape, its nodes, and the slot its copies read.
   cudaGraph_t graph = nullptr;
@@ -107,10 +110,11 @@ cudaError_t build(isp_b200_batch* b, const Slot& slot, Shape* shape) {
     const bool malvar = p.demosaic == ISP_DEMOSAIC_MALVAR;
     const bool sharpen = p.sharpen > 0.0F;
     f.variant = (malvar ? 1 : 0) | (sharpen ? 2 : 0) | ((e.raw.pattern >> 1) << 2);
-    f.tiles = main_kernel_tiles(e.raw.width, e.raw.height, &f.tiles_x);
+    f.tiles = main_kernel_tiles(e.raw.width, e.raw.height, &f.tiles_x, b->tile_rows);
     f.tile_begin = tiles;
     tiles += f.tiles;
-    const bool tma_main = encode_raw_map(f.desc, main_box_row_bytes(e.raw.format), main_box_rows(sharpen), &f.main_map);
+    const bool tma_main = encode_raw_map(f.desc, main_box_row_bytes(e.raw.format), main_box_rows(sharpen, b->tile_rows),
+                                         &f.main_map);
     bool tma_awb = true;
     if (f.desc.auto_wb) {
       f.awb_tiles = awb_kernel_tiles(e.raw.width, e.raw.height, &f.awb_tiles_x);
@@ -123,8 +127,8 @@ cudaError_t build(isp_b200_batch* b, const Slot& slot, Shape* shape) {
   }
   // CTAs: as many as fit (or the tuned count) per SM, never more than items.
   int bpsm = 0;
-  const size_t smem = batch_kernel_smem(lut_smem);
-  error = blocks_per_sm(dev, batch_kernel(lut_smem), smem, smem, &bpsm);
+  const size_t smem = batch_kernel_smem(lut_smem, b->tile_rows);
+  error = blocks_per_sm(dev, batch_kernel(lut_smem, b->tile_rows), smem, smem, &bpsm);
   if (error != cudaSuccess) return error;
   if (b->ctas_per_sm > 0) bpsm = std::min(bpsm, b->ctas_per_sm);
   const int main_ctas = std::max(1, std::min({tiles, dev.sm_count * bpsm, b->max_ctas}));
@@ -155,6 +159,7 @@ cudaError_t build(isp_b200_batch* b, const Slot& slot, Shape* shape) {
   shape->main_ctas = main_ctas;
   shape->awb_ctas = awb_ctas;
   shape->lut_smem = lut_smem;
+  shape->tile_rows = b->tile_rows;
   return cudaSuccess;
 }
 
@@ -210,14 +215,14 @@ cudaError_t enqueue(isp_b200_batch* b, const Slot& slot, const Shape& s, cudaStr
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(s.main_ctas);
   cfg.blockDim = dim3(kernel_threads());
-  cfg.dynamicSmemBytes = batch_kernel_smem(s.lut_smem);
+  cfg.dynamicSmemBytes = batch_kernel_smem(s.lut_smem, s.tile_rows);
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = s.awb_ctas > 0 ? 1 : 0;
-  return cudaLaunchKernelExC(&cfg, batch_kernel(s.lut_smem), args);
+  return cudaLaunchKernelExC(&cfg, batch_kernel(s.lut_smem, s.tile_rows), args);
 }
 
 // Builds the graph of a shape: the descriptor staging, then the passes.
@@ -248,10 +253,10 @@ cudaError_t make_graph(isp_b200_batch* b, const Slot& slot, const Shape& s) {
   }
   void* args[] = {&b->d_frames, &nframes, &b->d_ranges};
   cudaKernelNodeParams kp{};
-  kp.func = const_cast<void*>(batch_kernel(s.lut_smem));
+  kp.func = const_cast<void*>(batch_kernel(s.lut_smem, s.tile_rows));
   kp.gridDim = dim3(s.main_ctas);
   kp.blockDim = dim3(kernel_threads());
-  kp.sharedMemBytes = static_cast<unsigned int>(batch_kernel_smem(s.lut_smem));
+  kp.sharedMemBytes = static_cast<unsigned int>(batch_kernel_smem(s.lut_smem, s.tile_rows));
   kp.kernelParams = args;
   cudaGraphNode_t main = nullptr;
   if (awb != nullptr) {
@@ -484,24 +489,30 @@ int isp_b200_batch_autotune(isp_b200_batch* b, void* stream_ptr) {
     if (c > 0.0F) lowest = std::min(lowest, c);
   }
   for (int v = 0; v < 4; ++v) b->weights[v] = cost[v] > 0.0F ? cost[v] / lowest : kDefaultWeights[v];
-  // 2. CTAs per SM for the whole batch.
+  // 2. Tile height (64 or 32 rows) and CTAs per SM for the whole batch.
   int best_cps = 0;
+  int best_rows = 64;
   float best_ms = 1e30F;
-  for (const int cps : {1, 2, 0}) {
-    b->ctas_per_sm = cps;
-    float fastest = 1e30F;
-    for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
-      save(true);
-      if (e == cudaSuccess) e = cudaEventRecord(t0, stream);
-      if (e == cudaSuccess && isp_b200_batch_launch(b, stream, 0) != ISP_OK) e = cudaErrorUnknown;
-      if (e == cudaSuccess) e = cudaEventRecord(t1, stream);
-      fastest = std::min(fastest, elapsed());
-    }
-    if (fastest < best_ms) {
-      best_ms = fastest;
-      best_cps = cps;
+  for (const int rows : {64, 32}) {
+    for (const int cps : {1, 2, 3, 0}) {
+      b->tile_rows = rows;
+      b->ctas_per_sm = cps;
+      float fastest = 1e30F;
+      for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+        save(true);
+        if (e == cudaSuccess) e = cudaEventRecord(t0, stream);
+        if (e == cudaSuccess && isp_b200_batch_launch(b, stream, 0) != ISP_OK) e = cudaErrorUnknown;
+        if (e == cudaSuccess) e = cudaEventRecord(t1, stream);
+        fastest = std::min(fastest, elapsed());
+      }
+      if (fastest < best_ms) {
+        best_ms = fastest;
+        best_cps = cps;
+        best_rows = rows;
+      }
     }
   }
+  b->tile_rows = best_rows;
   b->ctas_per_sm = best_cps;
   save(true);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -524,6 +535,8 @@ int isp_b200_batch_info(const isp_b200_batch* b, isp_batch_info_c* info) {
   info->graph_replays = b->replays;
   info->graph_main_ctas = b->graph_shape.main_ctas;
   info->graph_awb_ctas = b->graph_shape.awb_ctas;
+  info->tile_rows = b->tile_rows;
+  info->block_threads = kernel_threads();
   clear_error();
   return ISP_OK;
 }
@@ -536,6 +549,14 @@ int isp_b200_batch_set_tuning(isp_b200_batch* b, const float weights[4], int32_t
   }
   b->ctas_per_sm = ctas_per_sm;
   b->tuned = true;
+  clear_error();
+  return ISP_OK;
+}
+
+int isp_b200_batch_set_tile_rows(isp_b200_batch* b, int32_t tile_rows) {
+  if (b == nullptr) return fail(ISP_EINVAL, "batch is null");
+  if (tile_rows_valid(tile_rows) == 0) return fail(ISP_EINVAL, "tile_rows must be 64 or 32");
+  b->tile_rows = tile_rows;
   clear_error();
   return ISP_OK;
 }

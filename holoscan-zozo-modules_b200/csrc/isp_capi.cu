@@ -258,7 +258,8 @@ cudaError_t blocks_per_sm(LaunchShapes& shapes, const void* kernel, size_t smem_
 }
 
 cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes& shapes, cudaStream_t stream,
-                         cudaEvent_t before_main, cudaEvent_t after_main, const char** step, bool after_previous) {
+                         cudaEvent_t before_main, cudaEvent_t after_main, const char** step, bool after_previous,
+                         int tile_rows) {
   *step = "launch";
   const int threads = kernel_threads();
   const int pattern = d.pattern;
@@ -301,21 +302,21 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
   const bool malvar = p.demosaic == ISP_DEMOSAIC_MALVAR;
   const bool sharpen = p.sharpen > 0.0F;
   // The tone table goes to shared memory when that still lets two CTAs share an SM.
-  const size_t without_lut = main_kernel_smem(sharpen, d.raw_format, 0);
-  const size_t with_lut = main_kernel_smem(sharpen, d.raw_format, d.tone_size);
+  const size_t without_lut = main_kernel_smem(sharpen, d.raw_format, 0, tile_rows);
+  const size_t with_lut = main_kernel_smem(sharpen, d.raw_format, d.tone_size, tile_rows);
   int lut_in_smem = d.tone_size <= kLutSmemEntries && with_lut <= kSmemPerTwoCtas ? 1 : 0;
   const size_t need = lut_in_smem ? with_lut : without_lut;
-  const void* k = main_kernel(malvar, sharpen, pattern, lut_in_smem != 0, d.out_format);
+  const void* k = main_kernel(malvar, sharpen, pattern, lut_in_smem != 0, d.out_format, tile_rows);
   // The instance's attribute covers its largest footprint (uint16 boxes, a
   // full shared tone table), so frames of any format can share it.
-  const size_t most = main_kernel_smem(sharpen, kRawU16, lut_in_smem ? kLutSmemEntries : 0);
+  const size_t most = main_kernel_smem(sharpen, kRawU16, lut_in_smem ? kLutSmemEntries : 0, tile_rows);
   int bpsm = 0;
   *step = "tile kernel attributes";
   if (const cudaError_t e = blocks_per_sm(shapes, k, most, need, &bpsm); e != cudaSuccess) return e;
   alignas(64) CUtensorMap map;
-  int use_tma = encode_raw_map(d, main_box_row_bytes(d.raw_format), main_box_rows(sharpen), &map) ? 1 : 0;
+  int use_tma = encode_raw_map(d, main_box_row_bytes(d.raw_format), main_box_rows(sharpen, tile_rows), &map) ? 1 : 0;
   int tiles_x = 0;
-  int tiles = main_kernel_tiles(d.width, d.height, &tiles_x);
+  int tiles = main_kernel_tiles(d.width, d.height, &tiles_x, tile_rows);
   const int blocks = std::min(tiles, shapes.sm_count * bpsm);
   FrameDesc desc = d;
   void* args[] = {&map, &desc, &tiles_x, &tiles, &use_tma, &lut_in_smem};
@@ -478,7 +479,7 @@ int isp_b200_process(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp
   }
   const char* step = "launch";
   error = launch_frame(d, pl->params.c, shapes, stream, pl->before_main, pl->after_main, &step,
-                       same_stream && pl->frame_overlap);
+                       same_stream && pl->frame_overlap, pl->rows_for(*raw));
   if (error == cudaSuccess) error = cudaGetLastError();
   if (error != cudaSuccess) return fail_cuda(error, (std::string("IspPipeline (cuda) ") + step).c_str());
   error = cudaEventRecord(pl->done, stream);
@@ -492,6 +493,79 @@ int isp_b200_process(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp
 int isp_b200_set_frame_overlap(isp_b200_pipeline* pl, int32_t enable) {
   if (pl == nullptr) return fail(ISP_EINVAL, "pipeline is null");
   pl->frame_overlap = enable != 0;
+  clear_error();
+  return ISP_OK;
+}
+
+int isp_b200_set_tile_rows(isp_b200_pipeline* pl, int32_t tile_rows) {
+  if (pl == nullptr) return fail(ISP_EINVAL, "pipeline is null");
+  if (tile_rows != 0 && tile_rows_valid(tile_rows) == 0) return fail(ISP_EINVAL, "tile_rows must be 0, 64 or 32");
+  pl->tile_rows = tile_rows;
+  clear_error();
+  return ISP_OK;
+}
+
+int isp_b200_autotune(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp_rgb_view_c* out,
+                      const isp_stats_c* stats, const isp_exposure_c* exposure, void* stream_ptr, int32_t* tile_rows) {
+  if (pl == nullptr || raw == nullptr || out == nullptr) return fail(ISP_EINVAL, "pipeline, raw or out is null");
+  std::string why = validate_raw(*raw, pl->params.c);
+  if (why.empty()) why = validate_out(*raw, *out);
+  if (!why.empty()) return fail(ISP_EINVAL, why);
+  auto stream = static_cast<cudaStream_t>(stream_ptr);
+  cudaError_t e = pl->queued ? cudaEventSynchronize(pl->done) : cudaSuccess;
+  // The white balance state, kept aside: the timed frames must leave no trace.
+  struct {
+    float g[3];
+    int v;
+  } saved{};
+  if (e == cudaSuccess) {
+    PrivateStream ps;
+    ps.copy(&saved, &pl->state.scratch->awb_gains[0], sizeof(saved), cudaMemcpyDeviceToHost);
+    e = ps.finish();
+  }
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&t0);
+  if (e == cudaSuccess) e = cudaEventCreate(&t1);
+  const int forced = pl->tile_rows;
+  int best_rows = 64;
+  float best_ms = 1e30F;
+  int status = ISP_OK;
+  for (const int rows : {64, 32}) {
+    pl->tile_rows = rows;
+    float fastest = 1e30F;
+    for (int rep = 0; rep < 4 && e == cudaSuccess && status == ISP_OK; ++rep) {
+      e = cudaEventRecord(t0, stream);
+      if (e == cudaSuccess) status = isp_b200_process(pl, raw, out, stats, exposure, stream_ptr);
+      if (e == cudaSuccess && status == ISP_OK) e = cudaEventRecord(t1, stream);
+      if (e == cudaSuccess && status == ISP_OK) e = cudaEventSynchronize(t1);
+      float ms = 0.0F;
+      if (e == cudaSuccess && status == ISP_OK) e = cudaEventElapsedTime(&ms, t0, t1);
+      if (rep > 0) fastest = std::min(fastest, ms);  // the first run warms up
+    }
+    if (fastest < best_ms) {
+      best_ms = fastest;
+      best_rows = rows;
+    }
+  }
+  pl->tile_rows = forced;
+  if (e == cudaSuccess && status == ISP_OK) {
+    e = cudaStreamSynchronize(stream);
+    PrivateStream ps;
+    ps.copy(&pl->state.scratch->awb_gains[0], &saved, sizeof(saved), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = ps.finish();
+  }
+  if (t0 != nullptr) cudaEventDestroy(t0);
+  if (t1 != nullptr) cudaEventDestroy(t1);
+  if (status != ISP_OK) return status;
+  if (e != cudaSuccess) return fail_cuda(e, "isp_b200_autotune");
+  int slot = -1;
+  for (int i = 0; i < pl->npicks && i < 8; ++i) {
+    const auto& k = pl->picks[i];
+    if (k.format == raw->format && k.width == raw->width && k.height == raw->height) slot = i;
+  }
+  if (slot < 0) slot = pl->npicks++ % 8;
+  pl->picks[slot] = {raw->format, raw->width, raw->height, best_rows};
+  if (tile_rows != nullptr) *tile_rows = best_rows;
   clear_error();
   return ISP_OK;
 }

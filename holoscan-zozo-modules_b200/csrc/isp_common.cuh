@@ -66,11 +66,16 @@ constexpr int kPW = 40;
 // Paired RGB columns (sharpening): pair q (0..33) holds pixels q - 1 and q + 31.
 constexpr int kCW2 = 34;
 
-template <bool kSharpen>
+// Tile heights the kernels are compiled for: kTH rows (the default) or
+// kTHShort rows (more, smaller tiles: a frame of few tiles spreads over more
+// SMs, and three CTAs share an SM).
+constexpr int kTHShort = 32;
+
+template <bool kSharpen, int kTileH = kTH>
 struct Geom {
   static constexpr int kHalo = kSharpen ? 4 : 2;  // sample rows above and below the tile
-  static constexpr int kSH = kTH + 2 * kHalo;
-  static constexpr int kCH = kTH + 2;  // RGB rows: y0 - 1 .. y0 + 64
+  static constexpr int kSH = kTileH + 2 * kHalo;
+  static constexpr int kCH = kTileH + 2;  // RGB rows: y0 - 1 .. y0 + kTileH
 };
 
 // ---- Shared memory layout -------------------------------------------------
@@ -90,10 +95,10 @@ struct Layout {
 
 __host__ __device__ constexpr int align128(int v) { return (v + 127) & ~127; }
 
-__host__ __device__ constexpr Layout layout_of(bool sharpen, int box_bytes_row, int lut_entries) {
+__host__ __device__ constexpr Layout layout_of(bool sharpen, int box_bytes_row, int lut_entries, int tile_h = kTH) {
   const int halo = sharpen ? 4 : 2;
-  const int sh = kTH + 2 * halo;
-  const int plane = align128((kTH + 2) * kCW2 * 8);
+  const int sh = tile_h + 2 * halo;
+  const int plane = align128((tile_h + 2) * kCW2 * 8);
   Layout l{};
   int o = 0;
   l.raw = o;

@@ -97,7 +97,8 @@ LaunchShapes& shapes_for_current_device(cudaError_t* error);
 // before_main / after_main (may be null) are recorded around the fused tile kernel.
 // `step` names the call that failed.
 cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes& shapes, cudaStream_t stream,
-                         cudaEvent_t before_main, cudaEvent_t after_main, const char** step, bool after_previous = false);
+                         cudaEvent_t before_main, cudaEvent_t after_main, const char** step, bool after_previous = false,
+                         int tile_rows = 64);
 
 }  // namespace isp_b200
 
@@ -110,6 +111,21 @@ struct isp_b200_pipeline {
   bool queued = false;
   cudaStream_t last_stream = nullptr;  // the stream of the last queued frame
   bool frame_overlap = true;           // isp_b200_set_frame_overlap
+  int tile_rows = 0;                   // isp_b200_set_tile_rows: 0 = per shape (isp_b200_autotune), else 64 / 32
+  struct ShapePick {
+    int32_t format, width, height, rows;
+  };
+  ShapePick picks[8] = {};  // isp_b200_autotune's choices, oldest replaced first
+  int npicks = 0;
+  // The tile height for a frame: the forced one, the shape's pick, else 64.
+  int rows_for(const isp_raw_view_c& raw) const {
+    if (tile_rows != 0) return tile_rows;
+    for (int i = 0; i < npicks && i < 8; ++i) {
+      const ShapePick& k = picks[i];
+      if (k.format == raw.format && k.width == raw.width && k.height == raw.height) return k.rows;
+    }
+    return 64;
+  }
   // Staging for isp_b200_process_host, grown on demand.
   cudaStream_t host_stream = nullptr;
   void* d_raw = nullptr;

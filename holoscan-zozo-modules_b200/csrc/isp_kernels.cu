@@ -31,31 +31,50 @@ const void* main_kernel_bn(int layout, bool lut_smem, int out_format);
 const void* main_kernel_bs(int layout, bool lut_smem, int out_format);
 const void* main_kernel_mn(int layout, bool lut_smem, int out_format);
 const void* main_kernel_ms(int layout, bool lut_smem, int out_format);
+const void* main_kernel_bn_short(int layout, bool lut_smem, int out_format);
+const void* main_kernel_bs_short(int layout, bool lut_smem, int out_format);
+const void* main_kernel_mn_short(int layout, bool lut_smem, int out_format);
+const void* main_kernel_ms_short(int layout, bool lut_smem, int out_format);
 const void* batch_kernel_shared_lut();
 const void* batch_kernel_global_lut();
+const void* batch_kernel_shared_lut_short();
+const void* batch_kernel_global_lut_short();
 
-const void* batch_kernel(bool lut_smem) { return lut_smem ? batch_kernel_shared_lut() : batch_kernel_global_lut(); }
+int tile_rows_valid(int tile_rows) { return tile_rows == kTH ? kTH : tile_rows == kTHShort ? kTHShort : 0; }
 
-const void* main_kernel(bool malvar, bool sharpen, int pattern, bool lut_smem, int out_format) {
+const void* batch_kernel(bool lut_smem, int tile_rows) {
+  if (tile_rows == kTHShort) return lut_smem ? batch_kernel_shared_lut_short() : batch_kernel_global_lut_short();
+  return lut_smem ? batch_kernel_shared_lut() : batch_kernel_global_lut();
+}
+
+const void* main_kernel(bool malvar, bool sharpen, int pattern, bool lut_smem, int out_format, int tile_rows) {
   // RGGB and BGGR share a layout (red/blue on the quad's diagonal), as do
   // GRBG and GBRG; the kernel swaps red and blue for BGGR and GBRG.
   const int layout = pattern >> 1;
+  if (tile_rows == kTHShort) {
+    if (malvar) {
+      return sharpen ? main_kernel_ms_short(layout, lut_smem, out_format)
+                     : main_kernel_mn_short(layout, lut_smem, out_format);
+    }
+    return sharpen ? main_kernel_bs_short(layout, lut_smem, out_format)
+                   : main_kernel_bn_short(layout, lut_smem, out_format);
+  }
   if (malvar) {
     return sharpen ? main_kernel_ms(layout, lut_smem, out_format) : main_kernel_mn(layout, lut_smem, out_format);
   }
   return sharpen ? main_kernel_bs(layout, lut_smem, out_format) : main_kernel_bn(layout, lut_smem, out_format);
 }
 
-size_t main_kernel_smem(bool sharpen, int raw_format, int lut_entries) {
-  return static_cast<size_t>(layout_of(sharpen, box_row_bytes(raw_format), lut_entries).total) + 128U;
+size_t main_kernel_smem(bool sharpen, int raw_format, int lut_entries, int tile_rows) {
+  return static_cast<size_t>(layout_of(sharpen, box_row_bytes(raw_format), lut_entries, tile_rows).total) + 128U;
 }
 
-int main_box_rows(bool sharpen) { return sharpen ? kTH + 8 : kTH + 4; }
+int main_box_rows(bool sharpen, int tile_rows) { return sharpen ? tile_rows + 8 : tile_rows + 4; }
 int main_box_row_bytes(int raw_format) { return box_row_bytes(raw_format); }
 
-int main_kernel_tiles(int width, int height, int* tiles_x) {
+int main_kernel_tiles(int width, int height, int* tiles_x, int tile_rows) {
   *tiles_x = (width + kTW - 1) / kTW;
-  return *tiles_x * ((height + kTH - 1) / kTH);
+  return *tiles_x * ((height + tile_rows - 1) / tile_rows);
 }
 
 int kernel_threads() { return kThreads; }

@@ -13,11 +13,14 @@ namespace isp_b200 {
 // (const CUtensorMap raw_map, FrameDesc, int tiles_x, int tiles, int use_tma,
 // int lut_in_smem). The raw map's box is main_box_row_bytes() bytes (or half
 // as many uint16 samples) by main_box_rows() rows.
-const void* main_kernel(bool malvar, bool sharpen, int pattern, bool lut_smem, int out_format);
-size_t main_kernel_smem(bool sharpen, int raw_format, int lut_entries);
-int main_box_rows(bool sharpen);
+// Each comes in two tile heights, tile_rows 64 (two CTAs per SM) or 32
+// (three CTAs per SM); tile_rows_valid() maps anything else to 0.
+const void* main_kernel(bool malvar, bool sharpen, int pattern, bool lut_smem, int out_format, int tile_rows = 64);
+size_t main_kernel_smem(bool sharpen, int raw_format, int lut_entries, int tile_rows = 64);
+int main_box_rows(bool sharpen, int tile_rows = 64);
 int main_box_row_bytes(int raw_format);
-int main_kernel_tiles(int width, int height, int* tiles_x);
+int main_kernel_tiles(int width, int height, int* tiles_x, int tile_rows = 64);
+int tile_rows_valid(int tile_rows);
 int kernel_threads();
 
 // The white balance statistics kernel; arguments (const CUtensorMap raw_map,
@@ -46,8 +49,8 @@ constexpr int kBatchLutEntries = 1024;
 // nframes, const int2* ranges), one range of work items per CTA. The tile
 // pass's dynamic shared memory is batch_kernel_smem(); the statistics pass's
 // is awb_kernel_smem().
-const void* batch_kernel(bool lut_smem);
-size_t batch_kernel_smem(bool lut_smem);
+const void* batch_kernel(bool lut_smem, int tile_rows = 64);
+size_t batch_kernel_smem(bool lut_smem, int tile_rows = 64);
 const void* awb_batch_kernel();
 // Descriptor staging (isp_batch.cu): arguments (const uint4* frames_src,
 // uint4* frames_dst, int frame_words, const uint4* ranges_src, uint4*

@@ -175,15 +175,15 @@ __device__ __forceinline__ void finish_row(const FrameDesc& p, const FrameSetup&
 // is waited for on `bar`); after phase A, when the box is free again,
 // `after_a()` runs (to prefetch the next tile). Adds the tile's statistics
 // sums and saturated count to `acc` (per thread).
-template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, class AfterA, int kOutSel = -1>
+template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, class AfterA, int kOutSel = -1, int kTileH = kTH>
 __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f, const TileSmem& m, int* minmax,
                                          int x0, int y0, bool use_tma, uint64_t* bar, uint32_t& phase,
                                          u64 (&acc)[4], AfterA after_a) {
-  using G = Geom<kSharpen>;
+  using G = Geom<kSharpen, kTileH>;
   constexpr int kPat = kLayout * 2;
   const int tid = threadIdx.x;
   const int box_bytes = box_row_bytes(p.raw_format);
-  const bool interior = x0 >= 4 && y0 >= G::kHalo && x0 + kSW - 4 <= p.width && y0 + kTH + G::kHalo <= p.height;
+  const bool interior = x0 >= 4 && y0 >= G::kHalo && x0 + kSW - 4 <= p.width && y0 + kTileH + G::kHalo <= p.height;
   TileCtx t;
   t.x0 = x0;
   t.y0 = y0;
@@ -205,11 +205,11 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
   // A. Samples of the tile and its halo, preprocessed once, as pairs.
   unsigned int saturated;
   if (!use_tma) {
-    saturated = phase_a2_fmt<2, G::kHalo>(p, t, m.P, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
+    saturated = phase_a2_fmt<2, G::kHalo, kTileH>(p, t, m.P, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
   } else if (interior) {
-    saturated = phase_a2_fmt<0, G::kHalo>(p, t, m.P, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
+    saturated = phase_a2_fmt<0, G::kHalo, kTileH>(p, t, m.P, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
   } else {
-    saturated = phase_a2_fmt<1, G::kHalo>(p, t, m.P, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
+    saturated = phase_a2_fmt<1, G::kHalo, kTileH>(p, t, m.P, box_bytes, f.qblack, f.qinv, f.qgain, f.want_stats);
   }
   acc[3] += saturated;
   __syncthreads();
@@ -218,7 +218,7 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
   // B. (Sharpening) RGB of the tile and its ring; BGGR and GBRG write the
   //    demosaic's red into the blue plane and its blue into the red.
   if constexpr (kSharpen) {
-    phase_b2<kMalvar, kPat>(m.P, f.swap_rb ? m.B : m.R, m.G, f.swap_rb ? m.R : m.B);
+    phase_b2<kMalvar, kPat, kTileH>(m.P, f.swap_rb ? m.B : m.R, m.G, f.swap_rb ? m.R : m.B);
     __syncthreads();
   }
 
@@ -226,7 +226,7 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
   //    of at most 2^20).
   unsigned int sums[3] = {0U, 0U, 0U};
   unsigned int npix = 0;
-  if constexpr (kSharpen && kOutSel >= 0) {
+  if constexpr (kSharpen && kOutSel >= 0 && kTileH == kTH) {
     // One unit per thread: output rows r and r + 1 of group uc, whose RGB
     // rows r .. r + 3 each plane loads once.
     int r, uc;
@@ -255,11 +255,12 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
     finish_row<kOutSel, kLutSmem>(p, f, m.hist, rgb0, x0 + 4 * uc, y0 + r, sums, npix);
     finish_row<kOutSel, kLutSmem>(p, f, m.hist, rgb1, x0 + 4 * uc, y0 + r + 1, sums, npix);
   } else {
-    // Two units of four pairs of one row per thread: sharpened (the batch
-    // kernel, whose output format is chosen per unit, keeps one call site of
-    // the finish), or demosaiced straight from the samples.
+    // Units of four pairs of one row, kTileH / 32 per thread: sharpened (the
+    // batch kernel, whose output format is chosen per unit, keeps one call
+    // site of the finish; and short tiles), or demosaiced straight from the
+    // samples.
 #pragma unroll 1
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < kTileH / 32; ++k) {
       int r, uc;
       unit_rc(tid + k * kThreads, true, r, uc);
       float2 rgb[4][3];
@@ -358,14 +359,15 @@ __device__ void flush_frame(const FrameDesc& p, const FrameSetup& f, const u64 (
   }
 }
 
-template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, int kOut>
-__global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_constant__ CUtensorMap map, FrameDesc p,
-                                                               int tiles_x, int tiles, int use_tma, int lut_in_smem) {
-  using G = Geom<kSharpen>;
+template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, int kOut, int kTileH>
+__global__ void __launch_bounds__(kThreads, kTileH == kTH ? 2 : 3)
+    isp_main_kernel(const __grid_constant__ CUtensorMap map, FrameDesc p, int tiles_x, int tiles, int use_tma,
+                    int lut_in_smem) {
+  using G = Geom<kSharpen, kTileH>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
   const int box_bytes = box_row_bytes(p.raw_format);
-  const TileSmem m = carve(smem, layout_of(kSharpen, box_bytes, kLutSmem ? p.tone_size : 0), G::kSH);
+  const TileSmem m = carve(smem, layout_of(kSharpen, box_bytes, kLutSmem ? p.tone_size : 0, kTileH), G::kSH);
   __shared__ uint64_t bar;
   __shared__ u64 red[4 * kWarps];
   __shared__ int minmax[2];
@@ -377,7 +379,7 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
   const auto issue = [&](int t) {
     const int ty = t / tiles_x;
     const int x0 = (t - ty * tiles_x) * kTW;
-    tma_load_2d(&map, m.box, &bar, box_x(fmt, x0), ty * kTH - G::kHalo, static_cast<unsigned int>(G::kSH * box_bytes));
+    tma_load_2d(&map, m.box, &bar, box_x(fmt, x0), ty * kTileH - G::kHalo, static_cast<unsigned int>(G::kSH * box_bytes));
   };
   // The first tile's box reads only the input frame: it is requested before
   // the wait below (the barrier initialised and made visible to the copy
@@ -425,7 +427,7 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
         }
       }
     };
-    run_tile<kMalvar, kSharpen, kLayout, kLutSmem, decltype(prefetch), kOut>(p, f, m, minmax, x0, ty * kTH,
+    run_tile<kMalvar, kSharpen, kLayout, kLutSmem, decltype(prefetch), kOut, kTileH>(p, f, m, minmax, x0, ty * kTileH,
                                                                              use_tma != 0, &bar, phase, acc, prefetch);
     ++done;
     tile = next_tile;  // written before run_tile's closing barrier
@@ -433,25 +435,26 @@ __global__ void __launch_bounds__(kThreads, 2) isp_main_kernel(const __grid_cons
   flush_frame(p, f, acc, m.hist, red, &last, done, static_cast<unsigned int>(tiles));
 }
 
-template <bool kMalvar, bool kSharpen, int kOut>
+template <bool kMalvar, bool kSharpen, int kOut, int kTileH>
 const void* main_instance_out(int layout, bool lut_smem) {
   if (layout == 0) {
-    return lut_smem ? reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 0, true, kOut>)
-                    : reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 0, false, kOut>);
+    return lut_smem ? reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 0, true, kOut, kTileH>)
+                    : reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 0, false, kOut, kTileH>);
   }
-  return lut_smem ? reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 1, true, kOut>)
-                  : reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 1, false, kOut>);
+  return lut_smem ? reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 1, true, kOut, kTileH>)
+                  : reinterpret_cast<const void*>(&isp_main_kernel<kMalvar, kSharpen, 1, false, kOut, kTileH>);
 }
 
-// The tile kernel for a layout, tone-table placement and output format (one
-// instance per format, so that each holds only its own store code).
-template <bool kMalvar, bool kSharpen>
+// The tile kernel of one tile height for a layout, tone-table placement and
+// output format (one instance per format, so that each holds only its own
+// store code).
+template <bool kMalvar, bool kSharpen, int kTileH>
 const void* main_instance(int layout, bool lut_smem, int out_format) {
   switch (out_format) {
-    case kOutRgb8: return main_instance_out<kMalvar, kSharpen, kOutRgb8>(layout, lut_smem);
-    case kOutRgba8: return main_instance_out<kMalvar, kSharpen, kOutRgba8>(layout, lut_smem);
-    case kOutRgb16: return main_instance_out<kMalvar, kSharpen, kOutRgb16>(layout, lut_smem);
-    default: return main_instance_out<kMalvar, kSharpen, kOutRgb32f>(layout, lut_smem);
+    case kOutRgb8: return main_instance_out<kMalvar, kSharpen, kOutRgb8, kTileH>(layout, lut_smem);
+    case kOutRgba8: return main_instance_out<kMalvar, kSharpen, kOutRgba8, kTileH>(layout, lut_smem);
+    case kOutRgb16: return main_instance_out<kMalvar, kSharpen, kOutRgb16, kTileH>(layout, lut_smem);
+    default: return main_instance_out<kMalvar, kSharpen, kOutRgb32f, kTileH>(layout, lut_smem);
   }
 }
 

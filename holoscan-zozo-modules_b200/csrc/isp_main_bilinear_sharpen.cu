@@ -1,10 +1,10 @@
-// isp_main_bilinear_sharpen.cu - instances of the fused tile kernel: bilinear demosaic, sharpening on.
+// isp_main_bilinear_sharpen.cu - instances of the fused tile kernel: bilinear demosaic, sharpening on, 64-row tiles.
 #include "isp_main.cuh"
 
 namespace isp_b200 {
 
 const void* main_kernel_bs(int layout, bool lut_smem, int out_format) {
-  return main_instance<false, true>(layout, lut_smem, out_format);
+  return main_instance<false, true, kTH>(layout, lut_smem, out_format);
 }
 
 }  // namespace isp_b200

@@ -1,10 +1,10 @@
-// isp_main_malvar.cu - instances of the fused tile kernel: Malvar-He-Cutler demosaic, sharpening off.
+// isp_main_malvar.cu - instances of the fused tile kernel: Malvar-He-Cutler demosaic, sharpening off, 64-row tiles.
 #include "isp_main.cuh"
 
 namespace isp_b200 {
 
 const void* main_kernel_mn(int layout, bool lut_smem, int out_format) {
-  return main_instance<true, false>(layout, lut_smem, out_format);
+  return main_instance<true, false, kTH>(layout, lut_smem, out_format);
 }
 
 }  // namespace isp_b200

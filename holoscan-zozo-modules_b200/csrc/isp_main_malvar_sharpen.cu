@@ -1,10 +1,10 @@
-// isp_main_malvar_sharpen.cu - instances of the fused tile kernel: Malvar-He-Cutler demosaic, sharpening on.
+// isp_main_malvar_sharpen.cu - instances of the fused tile kernel: Malvar-He-Cutler demosaic, sharpening on, 64-row tiles.
 #include "isp_main.cuh"
 
 namespace isp_b200 {
 
 const void* main_kernel_ms(int layout, bool lut_smem, int out_format) {
-  return main_instance<true, true>(layout, lut_smem, out_format);
+  return main_instance<true, true, kTH>(layout, lut_smem, out_format);
 }
 
 }  // namespace isp_b200

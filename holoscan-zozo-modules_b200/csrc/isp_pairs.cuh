@@ -53,11 +53,11 @@ __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); 
 //    of the tile's own samples (raw >= white, isp_math.hpp:316), each counted
 //    once. kSrc: 0 interior tile from the TMA box, 1 edge tile from the box
 //    (mirrored columns), 2 no box (global loads, mirrored).
-template <int kFmt, int kSrc, int kHalo>
+template <int kFmt, int kSrc, int kHalo, int kTileH>
 __device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileCtx& t, float2* P, int box_bytes,
                                                  const float (&qblack)[4], const float (&qinv)[4],
                                                  const float (&qgain)[4], bool want_stats) {
-  constexpr int kSH = kTH + 2 * kHalo;
+  constexpr int kSH = kTileH + 2 * kHalo;
   const unsigned int white = static_cast<unsigned int>(p.white);
   unsigned int saturated = 0;
   for (int unit = threadIdx.x; unit < kUnitsA * kSH; unit += kThreads) {
@@ -85,7 +85,7 @@ __device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileC
     }
     // Tile samples are s = 4 .. 67: the left lanes of units 1..8 hold 4..35,
     // their right lanes 36..67.
-    if (want_stats && j >= kHalo && j < kHalo + kTH && u >= 1 && u <= kHalf / 4) {
+    if (want_stats && j >= kHalo && j < kHalo + kTileH && u >= 1 && u <= kHalf / 4) {
       const int y = t.y0 + j - kHalo;
       const int xl = t.x0 + 4 * (u - 1);
       if (y < p.height) {
@@ -143,17 +143,17 @@ __device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileC
   return saturated;
 }
 
-template <int kSrc, int kHalo>
+template <int kSrc, int kHalo, int kTileH>
 __device__ __forceinline__ unsigned int phase_a2_fmt(const FrameDesc& p, const TileCtx& t, float2* P, int box_bytes,
                                                      const float (&qblack)[4], const float (&qinv)[4],
                                                      const float (&qgain)[4], bool want_stats) {
   // Global loads (no TMA box) read the format at run time in load_raw.
-  if constexpr (kSrc == 2) return phase_a2<kRawU8, kSrc, kHalo>(p, t, P, box_bytes, qblack, qinv, qgain, want_stats);
+  if constexpr (kSrc == 2) return phase_a2<kRawU8, kSrc, kHalo, kTileH>(p, t, P, box_bytes, qblack, qinv, qgain, want_stats);
   switch (p.raw_format) {
-    case kRawU8: return phase_a2<kRawU8, kSrc, kHalo>(p, t, P, box_bytes, qblack, qinv, qgain, want_stats);
-    case kRawU16: return phase_a2<kRawU16, kSrc, kHalo>(p, t, P, box_bytes, qblack, qinv, qgain, want_stats);
-    case kRawRaw10: return phase_a2<kRawRaw10, kSrc, kHalo>(p, t, P, box_bytes, qblack, qinv, qgain, want_stats);
-    default: return phase_a2<kRawRaw12, kSrc, kHalo>(p, t, P, box_bytes, qblack, qinv, qgain, want_stats);
+    case kRawU8: return phase_a2<kRawU8, kSrc, kHalo, kTileH>(p, t, P, box_bytes, qblack, qinv, qgain, want_stats);
+    case kRawU16: return phase_a2<kRawU16, kSrc, kHalo, kTileH>(p, t, P, box_bytes, qblack, qinv, qgain, want_stats);
+    case kRawRaw10: return phase_a2<kRawRaw10, kSrc, kHalo, kTileH>(p, t, P, box_bytes, qblack, qinv, qgain, want_stats);
+    default: return phase_a2<kRawRaw12, kSrc, kHalo, kTileH>(p, t, P, box_bytes, qblack, qinv, qgain, want_stats);
   }
 }
 
@@ -164,10 +164,10 @@ __device__ __forceinline__ unsigned int phase_a2_fmt(const FrameDesc& p, const T
 //    With swap_rb the demosaic's red and blue go to the other planes: the
 //    demosaic runs as the layout's canonical pattern (RGGB or GRBG), and
 //    BGGR and GBRG trade red and blue.
-template <bool kMalvar, int kPat>
+template <bool kMalvar, int kPat, int kTileH>
 __device__ __forceinline__ void phase_b2(const float2* P, float2* R, float2* G, float2* B) {
-  constexpr int kUnitsQ = kCW2 / 2;        // 17
-  constexpr int kUnits = (kTH + 2) / 2 * kUnitsQ;  // 33 x 17
+  constexpr int kUnitsQ = kCW2 / 2;                   // 17
+  constexpr int kUnits = (kTileH + 2) / 2 * kUnitsQ;  // 33 x 17 for 64 rows
   for (int unit = threadIdx.x; unit < kUnits; unit += kThreads) {
     const int ur = unit / kUnitsQ;
     const int uq = unit - ur * kUnitsQ;

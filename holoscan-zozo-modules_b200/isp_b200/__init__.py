@@ -85,6 +85,10 @@ def lib() -> C.CDLL:
         L.isp_b200_batch_autotune.argtypes = [C.c_void_p, C.c_void_p]
         L.isp_b200_batch_set_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
         L.isp_b200_batch_info.argtypes = [C.c_void_p, P(abi.BatchInfoC)]
+        L.isp_b200_batch_set_tile_rows.argtypes = [C.c_void_p, C.c_int32]
+        L.isp_b200_set_tile_rows.argtypes = [C.c_void_p, C.c_int32]
+        L.isp_b200_autotune.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC), P(abi.ExposureC),
+                                        C.c_void_p, P(C.c_int32)]
         L.isp_b200_server_config_default.argtypes = [P(abi.ServerConfigC)]
         L.isp_b200_server_create.argtypes = [P(abi.ServerConfigC), P(C.c_void_p)]
         L.isp_b200_server_add_stream.argtypes = [C.c_void_p, P(abi.ParamsC), P(abi.ServerStreamC), P(C.c_int32)]
@@ -198,6 +202,21 @@ class Pipeline:
         check(lib().isp_b200_device_status(self.handle, C.byref(v)))
         return int(v.value)
 
+    def set_tile_rows(self, tile_rows: int) -> None:
+        """0 (default): the height autotune picked for the frame's shape, else 64; 64 or 32 force it."""
+        check(lib().isp_b200_set_tile_rows(self.handle, tile_rows))
+
+    def autotune(self, raw: abi.RawViewC, out: abi.RgbViewC, histogram_ptr: int = 0, stats_ptr: int = 0,
+                 exposure: Tuple[int, float] = (0, 0.0), stream: int = 0) -> int:
+        """Times both tile heights on this frame (device buffers), keeps the faster for its raw format and
+        size, restores the white balance state; returns the chosen rows."""
+        st = abi.StatsC(histogram_ptr or None, stats_ptr or None)
+        exp = abi.ExposureC(exposure[0], exposure[1])
+        rows = C.c_int32()
+        check(lib().isp_b200_autotune(self.handle, C.byref(raw), C.byref(out), C.byref(st), C.byref(exp),
+                                      stream or None, C.byref(rows)))
+        return int(rows.value)
+
     def set_frame_overlap(self, enable: bool) -> None:
         """On (default): a frame queued right behind the previous one on the same stream starts its statistics
         pass while that frame's tile pass finishes."""
@@ -281,12 +300,16 @@ class Batch:
         w = (C.c_float * 4)(*weights)
         check(lib().isp_b200_batch_set_tuning(self.handle, w, ctas_per_sm))
 
+    def set_tile_rows(self, tile_rows: int) -> None:
+        """The tile pass's tile height for later launches: 64 or 32 rows."""
+        check(lib().isp_b200_batch_set_tile_rows(self.handle, tile_rows))
+
     def info(self) -> dict:
         i = abi.BatchInfoC()
         check(lib().isp_b200_batch_info(self.handle, C.byref(i)))
         return {"frames": i.frames, "weights": list(i.weights), "ctas_per_sm": i.ctas_per_sm, "tuned": bool(i.tuned),
                 "graph_replays": i.graph_replays, "graph_main_ctas": i.graph_main_ctas,
-                "graph_awb_ctas": i.graph_awb_ctas}
+                "graph_awb_ctas": i.graph_awb_ctas, "tile_rows": i.tile_rows, "block_threads": i.block_threads}
 
 
 class Server:

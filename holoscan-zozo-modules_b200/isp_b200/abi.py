@@ -100,7 +100,8 @@ class ExposureC(C.Structure):
 
 class BatchInfoC(C.Structure):
     _fields_ = [("frames", C.c_int32), ("weights", C.c_float * 4), ("ctas_per_sm", C.c_int32), ("tuned", C.c_int32),
-                ("graph_replays", C.c_int32), ("graph_main_ctas", C.c_int32), ("graph_awb_ctas", C.c_int32)]
+                ("graph_replays", C.c_int32), ("graph_main_ctas", C.c_int32), ("graph_awb_ctas", C.c_int32),
+                ("tile_rows", C.c_int32), ("block_threads", C.c_int32)]
 
 
 class ServerConfigC(C.Structure):

@@ -212,6 +212,8 @@ typedef struct isp_batch_info_c {
   int32_t graph_replays;
   int32_t graph_main_ctas;
   int32_t graph_awb_ctas;
+  int32_t tile_rows;     /* the tile pass's tile height: 64 or 32 */
+  int32_t block_threads; /* threads per CTA of both passes */
 } isp_batch_info_c;
 
 /* A batch of up to `capacity` frames on the current device. */
@@ -235,6 +237,10 @@ ISP_B200_API int isp_b200_batch_autotune(isp_b200_batch* batch, void* stream);
 /* Sets the tuning by hand: weights per variant, CTAs per SM (0: all that fit). */
 ISP_B200_API int isp_b200_batch_set_tuning(isp_b200_batch* batch, const float weights[4], int32_t ctas_per_sm);
 ISP_B200_API int isp_b200_batch_info(const isp_b200_batch* batch, isp_batch_info_c* info);
+/* The tile pass's tile height for later launches: 64 (two CTAs per SM) or
+ * 32 rows (three CTAs per SM, more and smaller work items); the autotuner
+ * picks it by timing both. ISP_EINVAL for any other value. */
+ISP_B200_API int isp_b200_batch_set_tile_rows(isp_b200_batch* batch, int32_t tile_rows);
 
 /* ---- Serving: many camera streams, continuous batching -----------------
  * No reference counterpart (the reference's operator runs one camera on one
@@ -416,6 +422,25 @@ ISP_B200_API int isp_b200_process_noalloc(const isp_params_c* params, const isp_
  * wait (*status 1: that frame's outputs are not trustworthy), else 0. Call it
  * before the next no-alloc call, which clears the flag. */
 ISP_B200_API int isp_b200_noalloc_status(void* stream, int32_t* status);
+
+/* Tile height of the fused tile pass, no reference counterpart (the
+ * reference's CUDA backend uses one 32x16 block shape, cuda_pipeline.cu:17-19).
+ * The pass is compiled for 64-row tiles (two CTAs per SM) and 32-row tiles
+ * (three CTAs per SM: a frame of few tiles spreads over more SMs). 0 (the
+ * default) uses the height isp_b200_autotune picked for the frame's raw
+ * format and size, else 64; 64 or 32 force it for every frame. Outputs are
+ * bit-identical either way. ISP_EINVAL for any other value. */
+ISP_B200_API int isp_b200_set_tile_rows(isp_b200_pipeline* pipeline, int32_t tile_rows);
+
+/* Tunes the tile height for one frame shape, no reference counterpart:
+ * processes `raw` into `out` (device buffers, as isp_b200_process) a few
+ * times with each tile height, keeps the faster for this raw format, width
+ * and height (up to 8 shapes per pipeline) and writes it to *tile_rows. The
+ * pipeline's white balance state is put back afterwards, so the frames it ran
+ * leave no trace; waits for `stream`. */
+ISP_B200_API int isp_b200_autotune(isp_b200_pipeline* pipeline, const isp_raw_view_c* raw, const isp_rgb_view_c* out,
+                                   const isp_stats_c* stats, const isp_exposure_c* exposure, void* stream,
+                                   int32_t* tile_rows);
 
 /* Frame overlap, no reference counterpart (on by default): when frames of
  * one pipeline follow each other on one stream, the next frame's white

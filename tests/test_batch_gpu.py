@@ -59,10 +59,12 @@ def _frames(round_):
     return [DeviceFrame(raw, spec[9], True) for raw, spec in zip(_frame_raws(round_), MIX)]
 
 
-def _run_batch(use_graph, rounds=2, tune=False):
+def _run_batch(use_graph, rounds=2, tune=False, tile_rows=0):
     torch = torch_cuda()
     cams = [isp_b200.Pipeline(_params(spec, i)) for i, spec in enumerate(MIX)]
     batch = isp_b200.Batch(len(MIX))
+    if tile_rows:
+        batch.set_tile_rows(tile_rows)
     stream = torch.cuda.Stream()
     results = []
     for r in range(rounds):
@@ -123,7 +125,14 @@ def test_batch_graph_replays_match_single_frames(single):
 
 def test_batch_after_autotune_matches(single):
     got, info = _run_batch(True, rounds=2, tune=True)
-    assert info["tuned"]
+    assert info["tuned"] and info["tile_rows"] in (64, 32) and info["block_threads"] == 256
+    _compare(got, single)
+
+
+@pytest.mark.parametrize("rows", [32, 64])
+def test_batch_each_tile_height_matches_single_frames(single, rows):
+    got, info = _run_batch(True, rounds=2, tile_rows=rows)
+    assert info["tile_rows"] == rows
     _compare(got, single)
 
 

@@ -40,6 +40,43 @@ def test_device_matches_reference(name):
     pipe.close()
 
 
+@pytest.mark.parametrize("name", CASES)
+def test_short_tiles_match_reference(name):
+    """Every golden fixture again through the 32-row tile pass (three CTAs per SM)."""
+    case = load_case(name)
+    pipe = isp_b200.Pipeline(case.params)
+    pipe.set_tile_rows(32)
+    for f, raw in enumerate(case.frame_raws()):
+        got = run_device(pipe, raw, case.out_format, case.with_stats, case.exposure)
+        _check(name, f, got, case.expected[f], case.with_stats)
+        gains, valid = pipe.awb()
+        assert np.array_equal(np.array([*gains.view(np.uint32), valid], np.uint32), case.expected[f]["awb"])
+    assert pipe.device_status() == 0
+    pipe.close()
+
+
+def test_autotune_picks_a_height_per_shape_and_leaves_no_trace():
+    """isp_b200_autotune times both tile heights on a frame, keeps the faster
+    for that shape and puts the white balance state back: the frames after it
+    are the reference's first frames, at whichever height it picked."""
+    torch = torch_cuda()
+    case = load_case("malvar_gray_world")
+    pipe = isp_b200.Pipeline(case.params)
+    stream = torch.cuda.Stream()
+    raws = case.frame_raws()
+    tune = DeviceFrame(raws[0], case.out_format, True)
+    rv, ov = tune.views()
+    rows = pipe.autotune(rv, ov, tune.hist.data_ptr(), tune.stats.data_ptr(), case.exposure, stream.cuda_stream)
+    assert rows in (64, 32)
+    assert pipe.awb()[1] == 0, "the white balance state is the fresh pipeline's again"
+    for f, raw in enumerate(raws):
+        got = run_device(pipe, raw, case.out_format, case.with_stats, case.exposure)
+        _check("malvar_gray_world", f, got, case.expected[f], case.with_stats)
+    with pytest.raises(ValueError, match="tile_rows"):
+        pipe.set_tile_rows(48)
+    pipe.close()
+
+
 @pytest.mark.parametrize("name", [n for n in CASES if not n.startswith(("sweep_", "edge_"))])
 def test_host_buffers_match_reference(name):
     case = load_case(name)
@@ -155,10 +192,12 @@ def full_size_frames():
     return frames
 
 
+@pytest.mark.parametrize("rows", [64, 32])
 @pytest.mark.parametrize("which", ["c0_1080p_u16_rggb_bilinear", "c1_4k_raw10_grbg_malvar_sharpen"])
-def test_full_size_configs_match_oracle(full_size_frames, which):
+def test_full_size_configs_match_oracle(full_size_frames, which, rows):
     w, raw = full_size_frames[which]
     pipe = isp_b200.Pipeline(w.params)
+    pipe.set_tile_rows(rows)
     ref = oracle.OraclePipeline(w.params)
     for f in range(2):  # two frames: the white balance smoothing runs too
         got = run_device(pipe, raw, w.out_format, True, (10_000_000, 2.0))
