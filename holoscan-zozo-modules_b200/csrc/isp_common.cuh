@@ -346,6 +346,69 @@ __device__ LscTile build_lsc(const FrameDesc& p, const float* grid, int pattern,
   return lt;
 }
 
+// build_lsc<true> for a tile none of whose rows and columns is mirrored:
+// the grid rows it spans follow from its first and last rows (a row's grid
+// cell never decreases down the frame), so the row maps and the paired table
+// are written in one pass behind one block barrier, each table entry working
+// out its own column's cell (the same operations as build_lsc's column maps).
+// Tiles whose table would not fit take build_lsc<true>. Of the column maps
+// only the columns themselves are written (the path of phase A without a TMA
+// box reads them); the cells are worked out where the table needs them.
+__device__ LscTile build_lsc_inner(const FrameDesc& p, const float* grid, int pattern, int x_first, int y_first,
+                                   int nrows, int* col_mx, int* col_ix, float* col_tx, int* row_my, int* row_k,
+                                   float* row_ty, float* table, int* minmax) {
+  LscTile lt{0, 0};
+  const int t = threadIdx.x;
+  if (p.lsc == nullptr) {
+    if (t < kSW) col_mx[t] = x_first + t;
+    if (t < nrows) row_my[t] = y_first + t;
+    __syncthreads();
+    return lt;
+  }
+  const auto row_cell = [&](int y) {
+    const int iy = static_cast<int>(static_cast<float>(y) * p.lsc_sy);
+    return iy > p.lsc_height - 2 ? p.lsc_height - 2 : iy;
+  };
+  lt.iy0 = row_cell(y_first);
+  lt.rows = row_cell(y_first + nrows - 1) - lt.iy0 + 2;
+  if (lt.rows > kLscTableRows) {
+    return build_lsc<true>(p, grid, pattern, x_first, kSW, y_first, nrows, false, 0, 0, col_mx, col_ix, col_tx, row_my,
+                           row_k, row_ty, table, minmax);
+  }
+  if (t < kSW) col_mx[t] = x_first + t;
+  if (t < nrows) {
+    const int y = y_first + t;
+    row_my[t] = y;
+    const float fy = static_cast<float>(y) * p.lsc_sy;
+    int iy = static_cast<int>(fy);
+    iy = iy > p.lsc_height - 2 ? p.lsc_height - 2 : iy;
+    row_k[t] = iy - lt.iy0;
+    row_ty[t] = fy - static_cast<float>(iy);
+  }
+  const int step = p.lsc_channels;
+  const int planes = step == 4 ? 2 : 1;
+  const auto entry = [&](int k, int par, int i) {
+    const int x = x_first + i;
+    const float fx = static_cast<float>(x) * p.lsc_sx;
+    int ix = static_cast<int>(fx);
+    ix = ix > p.lsc_width - 2 ? p.lsc_width - 2 : ix;
+    const float tx = fx - static_cast<float>(ix);
+    const int ch = step == 4 ? cfa_of(pattern, (par << 1) | (x & 1)) : 0;
+    const float* g = grid + ((lt.iy0 + k) * p.lsc_width + ix) * step + ch;
+    return g[0] + (g[step] - g[0]) * tx;
+  };
+  float2* table2 = reinterpret_cast<float2*>(table);
+  for (int e = t; e < lt.rows * planes * kPW; e += kThreads) {
+    const int i = e % kPW;
+    const int kp = e / kPW;
+    const int par = kp % planes;
+    const int k = kp / planes;
+    table2[(k * 2 + par) * kPW + i] = make_float2(entry(k, par, i), entry(k, par, i + kHalf));
+  }
+  __syncthreads();
+  return lt;
+}
+
 __device__ __forceinline__ u64 warp_sum(u64 v) {
 #pragma unroll
   for (int offset = 16; offset > 0; offset >>= 1) v += __shfl_down_sync(0xFFFFFFFFU, v, offset);

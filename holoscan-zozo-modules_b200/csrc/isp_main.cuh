@@ -194,9 +194,11 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
   t.row_ty = m.row_ty;
   t.table = m.table;
   t.grid = f.grid;
-  t.lt = build_lsc<true>(p, f.grid, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, !interior, p.width + 3,
-                         p.height + G::kHalo - 1, m.col_mx, m.col_ix, m.col_tx, m.row_my, m.row_k, m.row_ty,
-                         reinterpret_cast<float*>(m.table), minmax);
+  t.lt = interior ? build_lsc_inner(p, f.grid, p.pattern, x0 - 4, y0 - G::kHalo, G::kSH, m.col_mx, m.col_ix,
+                                    m.col_tx, m.row_my, m.row_k, m.row_ty, reinterpret_cast<float*>(m.table), minmax)
+                  : build_lsc<true>(p, f.grid, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, true, p.width + 3,
+                                    p.height + G::kHalo - 1, m.col_mx, m.col_ix, m.col_tx, m.row_my, m.row_k, m.row_ty,
+                                    reinterpret_cast<float*>(m.table), minmax);
   if (use_tma) {
     if (!mbar_wait(bar, phase) && tid == 0) report_wait_timeout(p.scratch);
     phase ^= 1U;
