@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_kernel(const __grid_const
   const float* grid = p.lsc;
   const int gains = p.lsc_width * p.lsc_height * p.lsc_channels;
   if (p.lsc != nullptr && gains <= kGridSmemGains) {
-    for (int i = tid; i < gains; i += kThreads) grid_s[i] = p.lsc[i];
+    for (int i = tid; i < gains; i += kThreads) cp_async4(&grid_s[i], &p.lsc[i]);
     grid = grid_s;
   }
   if (tid == 0 && use_tma) {
@@ -143,7 +143,8 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_kernel(const __grid_const
     tma_load_2d(&map, boxes + b * 64 * 128, &bars[b], awb_box_x(p.raw_format, x0), ty * 64,
                 static_cast<unsigned int>(kBoxRows * box_bytes));
   };
-  __syncthreads();  // barriers initialised
+  cp_async_wait_all();
+  __syncthreads();  // barriers initialised, the gains in shared memory
   if (use_tma && tid == 0 && ty0 < ty1) issue(ty0, 0);
   // The band's maps and table (block-synchronised inside), while the first
   // box is in flight.

@@ -183,6 +183,20 @@ __device__ __forceinline__ void report_wait_timeout(Scratch* s) { atomicExch(&s-
 
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// Copies of 4 or 8 bytes from global to shared memory that bypass the
+// registers: a thread's copies are all in flight at once (a fill loop of
+// plain loads and stores waits out one L2 round trip per iteration), and
+// cp_async_wait_all() returns once this thread's copies have landed.
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // The TMA coordinates of the box for a tile at (x0, y0) (x in the tensor's
 // elements: bytes, or uint16 samples), 16-byte aligned for any x0 % 64 == 0.
 __device__ __forceinline__ int box_x(int fmt, int x0) {

@@ -67,15 +67,17 @@ struct FrameSetup {
 
 // The frame's shared-memory copies: the lens shading gains (when they fit),
 // the tone table (kLutSmem) and the cleared block histogram. They read only
-// the pipeline's own tables, never what the statistics pass writes.
+// the pipeline's own tables, never what the statistics pass writes. The
+// tables arrive by asynchronous copies: each thread calls cp_async_wait_all()
+// before the block barrier that publishes them.
 template <bool kLutSmem>
 __device__ __forceinline__ void fill_frame_smem(const FrameDesc& p, const TileSmem& m) {
   const int gains = p.lsc_width * p.lsc_height * p.lsc_channels;
   if (p.lsc != nullptr && gains <= kGridSmemGains) {
-    for (int i = threadIdx.x; i < gains; i += kThreads) m.grid[i] = p.lsc[i];
+    for (int i = threadIdx.x; i < gains; i += kThreads) cp_async4(&m.grid[i], &p.lsc[i]);
   }
   if constexpr (kLutSmem) {
-    for (int i = threadIdx.x; i < p.tone_size; i += kThreads) m.lut_s[i] = p.tone[i];
+    for (int i = threadIdx.x; i < p.tone_size; i += kThreads) cp_async8(&m.lut_s[i], &p.tone[i]);
   }
   if (p.hist_out != nullptr) {
     for (int i = threadIdx.x; i < kHistChannels * kHistBins; i += kThreads) m.hist[i] = 0U;
@@ -83,9 +85,9 @@ __device__ __forceinline__ void fill_frame_smem(const FrameDesc& p, const TileSm
 }
 
 // Reads the frame's gains (its estimate, for auto white balance) and, with
-// kFill, fills the frame's shared memory (fill_frame_smem; without it the
-// caller did so before). The caller synchronises the block before the first
-// tile.
+// kFill, fills the frame's shared memory (fill_frame_smem, its copies waited
+// for; without kFill the caller filled it before and waits for the copies).
+// The caller synchronises the block before the first tile.
 template <bool kLutSmem, bool kFill = true>
 __device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const TileSmem& m) {
   if constexpr (kFill) fill_frame_smem<kLutSmem>(p, m);
@@ -109,6 +111,7 @@ __device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const Tile
   f.swap_rb = (p.pattern & 1) != 0;
   f.want_hist = p.hist_out != nullptr;
   f.want_stats = p.stats_out != nullptr;
+  if constexpr (kFill) cp_async_wait_all();
   return f;
 }
 
@@ -175,10 +178,16 @@ __device__ __forceinline__ void finish_row(const FrameDesc& p, const FrameSetup&
 // is waited for on `bar`); after phase A, when the box is free again,
 // `after_a()` runs (to prefetch the next tile). Adds the tile's statistics
 // sums and saturated count to `acc` (per thread).
-template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, class AfterA, int kOutSel = -1, int kTileH = kTH>
+// A hook that does nothing (run_tile's before_c by default).
+struct NoHook {
+  __device__ __forceinline__ void operator()() const {}
+};
+
+template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, class AfterA, int kOutSel = -1, int kTileH = kTH,
+          class BeforeC = NoHook>
 __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f, const TileSmem& m, int* minmax,
                                          int x0, int y0, bool use_tma, uint64_t* bar, uint32_t& phase,
-                                         u64 (&acc)[4], AfterA after_a) {
+                                         u64 (&acc)[4], AfterA after_a, BeforeC before_c = BeforeC{}) {
   using G = Geom<kSharpen, kTileH>;
   constexpr int kPat = kLayout * 2;
   const int tid = threadIdx.x;
@@ -223,6 +232,7 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
     phase_b2<kMalvar, kPat, kTileH>(m.P, f.swap_rb ? m.B : m.R, m.G, f.swap_rb ? m.R : m.B);
     __syncthreads();
   }
+  before_c();
 
   // C. The statistics sums stay below 2^32 per thread and tile (16 pixels
   //    of at most 2^20).
@@ -404,6 +414,7 @@ __global__ void __launch_bounds__(kThreads, kTileH == kTH ? 2 : 3)
   // estimate touches the white balance state read below.
   griddep_launch_dependents();
   const FrameSetup f = setup_frame<kLutSmem, false>(p, m);
+  cp_async_wait_all();
   __syncthreads();
 
   u64 acc[4] = {0, 0, 0, 0};  // linear R, G, B in 2^-20 units; saturated samples
@@ -416,11 +427,15 @@ __global__ void __launch_bounds__(kThreads, kTileH == kTH ? 2 : 3)
   while (tile < tiles) {
     const int ty = tile / tiles_x;
     const int x0 = (tile - ty * tiles_x) * kTW;
-    // The CTA's next tile, claimed now; its box is requested once this
-    // tile's box is free (after phase A), to arrive during B and C.
+    // The CTA's next tile. With sharpening it is claimed once this tile's
+    // box is free (after phase A) and its box requested before phase C (the
+    // claim's round trip hidden behind phase B, the copy behind phase C), so
+    // that claims are made as late as the box allows and the frame's last
+    // tiles go to the CTAs that are free first; without sharpening (no phase
+    // B) it is claimed at the tile's start and its box requested after A.
     unsigned int claim = 0;
-    if (threadIdx.x == 0) claim = gridDim.x + atomicAdd(&p.scratch->tile_next, 1U);
-    const auto prefetch = [&] {
+    if (!kSharpen && threadIdx.x == 0) claim = gridDim.x + atomicAdd(&p.scratch->tile_next, 1U);
+    const auto request = [&] {
       if (threadIdx.x == 0) {
         next_tile = static_cast<int>(claim);
         if (use_tma && static_cast<int>(claim) < tiles) {
@@ -429,8 +444,18 @@ __global__ void __launch_bounds__(kThreads, kTileH == kTH ? 2 : 3)
         }
       }
     };
-    run_tile<kMalvar, kSharpen, kLayout, kLutSmem, decltype(prefetch), kOut, kTileH>(p, f, m, minmax, x0, ty * kTileH,
-                                                                             use_tma != 0, &bar, phase, acc, prefetch);
+    const auto after_a = [&] {
+      if constexpr (kSharpen) {
+        if (threadIdx.x == 0) claim = gridDim.x + atomicAdd(&p.scratch->tile_next, 1U);
+      } else {
+        request();
+      }
+    };
+    const auto before_c = [&] {
+      if constexpr (kSharpen) request();
+    };
+    run_tile<kMalvar, kSharpen, kLayout, kLutSmem, decltype(after_a), kOut, kTileH, decltype(before_c)>(
+        p, f, m, minmax, x0, ty * kTileH, use_tma != 0, &bar, phase, acc, after_a, before_c);
     ++done;
     tile = next_tile;  // written before run_tile's closing barrier
   }
