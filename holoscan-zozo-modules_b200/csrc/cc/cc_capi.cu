@@ -7,6 +7,7 @@
 #include <string>
 
 #include "../isp_host.hpp"
+#include "../isp_trace.hpp"
 #include "cc_common.cuh"
 
 extern "C" {
@@ -16,6 +17,7 @@ extern "C" {
 // device, checked, planned, one kernel launched.
 ISP_B200_API int cc_b200_convert(const cc_image_c* source, const cc_image_c* destination, const cc_params_c* params,
                                  void* stream) {
+  const isp_b200::TraceRange range("cc.convert", isp_b200::kTraceKernel);
   isp_b200::clear_error();
   if (source == nullptr || destination == nullptr || params == nullptr) {
     return isp_b200::fail(ISP_EINVAL, "null argument");

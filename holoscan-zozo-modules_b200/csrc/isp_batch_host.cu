@@ -24,6 +24,7 @@
 #include "isp_b200.h"
 #include "isp_host.hpp"
 #include "isp_kernels.cuh"
+#include "isp_trace.hpp"
 
 using namespace isp_b200;
 
@@ -371,6 +372,7 @@ int isp_b200_batch_launch(isp_b200_batch* b, void* stream_ptr, int32_t use_graph
     clear_error();
     return ISP_OK;
   }
+  const TraceRange range("isp.batch.launch");
   auto stream = static_cast<cudaStream_t>(stream_ptr);
   Slot& slot = b->slots[b->next_slot];
   // The slot's previous contents must have reached the device.
@@ -381,7 +383,11 @@ int isp_b200_batch_launch(isp_b200_batch* b, void* stream_ptr, int32_t use_graph
   }
   static_cast<void>(cudaGetLastError());
   Shape shape;
-  cudaError_t e = build(b, slot, &shape);
+  cudaError_t e = cudaSuccess;
+  {
+    const TraceRange build_range("isp.batch.build", kTraceCopy);
+    e = build(b, slot, &shape);
+  }
   if (e != cudaSuccess) return fail_cuda(e, "batch build");
   for (const Entry& en : b->entries) {
     if (en.camera->queued) {
@@ -402,12 +408,14 @@ int isp_b200_batch_launch(isp_b200_batch* b, void* stream_ptr, int32_t use_graph
       if (e != cudaSuccess) return fail_cuda(e, "batch graph");
     }
     // The staging reads this launch's slot.
+    const TraceRange replay("isp.batch.replay", kTraceKernel);
     StageArgs stage(b, slot, shape);
     cudaKernelNodeParams sp = stage.node();
     e = cudaGraphExecKernelNodeSetParams(b->exec, b->stage, &sp);
     if (e == cudaSuccess) e = cudaGraphLaunch(b->exec, stream);
     if (e == cudaSuccess) ++b->replays;
   } else {
+    const TraceRange kernels("isp.batch.enqueue", kTraceKernel);
     e = enqueue(b, slot, shape, stream);
   }
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -427,6 +435,7 @@ int isp_b200_batch_launch(isp_b200_batch* b, void* stream_ptr, int32_t use_graph
 
 int isp_b200_batch_autotune(isp_b200_batch* b, void* stream_ptr) {
   if (b == nullptr) return fail(ISP_EINVAL, "batch is null");
+  const TraceRange range("isp.batch.autotune");
   if (b->entries.empty()) return fail(ISP_EINVAL, "batch is empty");
   auto stream = static_cast<cudaStream_t>(stream_ptr);
   const int n = static_cast<int>(b->entries.size());

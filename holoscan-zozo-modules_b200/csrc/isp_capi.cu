@@ -22,6 +22,7 @@
 #include "isp_b200.h"
 #include "isp_host.hpp"
 #include "isp_kernels.cuh"
+#include "isp_trace.hpp"
 
 namespace isp_b200 {
 
@@ -279,6 +280,7 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
     FrameDesc desc = d;
     void* args[] = {&map, &desc, &strips, &tiles_y, &band_tiles, &use_tma};
     *step = "white balance kernel launch";
+    const TraceRange range("isp.statistics_pass", kTraceKernel);
     // With after_previous, as a programmatic dependent of the kernel queued
     // just before it (the previous frame's tile pass, when frames follow each
     // other on one stream): its CTAs sum this frame's raw samples on the SMs
@@ -325,6 +327,7 @@ cudaError_t launch_frame(const FrameDesc& d, const isp_params_c& p, LaunchShapes
     if (e != cudaSuccess) return e;
   }
   *step = "tile kernel launch";
+  const TraceRange range("isp.tile_pass", kTraceKernel);
   // After the statistics pass, as its programmatic dependent: the tile pass
   // becomes resident on the SMs the statistics pass leaves and waits in the
   // kernel (griddepcontrol.wait) for its completion before anything else. An
@@ -458,6 +461,7 @@ int isp_b200_awb_state(isp_b200_pipeline* pl, float gains[3], int32_t* valid) {
 int isp_b200_process(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp_rgb_view_c* out,
                      const isp_stats_c* stats, const isp_exposure_c* exposure, void* stream_ptr) {
   if (pl == nullptr || raw == nullptr || out == nullptr) return fail(ISP_EINVAL, "pipeline, raw or out is null");
+  const TraceRange range("isp.process");
   std::string why = validate_raw(*raw, pl->params.c);
   if (why.empty()) why = validate_out(*raw, *out);
   if (!why.empty()) return fail(ISP_EINVAL, why);
@@ -508,6 +512,7 @@ int isp_b200_set_tile_rows(isp_b200_pipeline* pl, int32_t tile_rows) {
 int isp_b200_autotune(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp_rgb_view_c* out,
                       const isp_stats_c* stats, const isp_exposure_c* exposure, void* stream_ptr, int32_t* tile_rows) {
   if (pl == nullptr || raw == nullptr || out == nullptr) return fail(ISP_EINVAL, "pipeline, raw or out is null");
+  const TraceRange range("isp.autotune");
   std::string why = validate_raw(*raw, pl->params.c);
   if (why.empty()) why = validate_out(*raw, *out);
   if (!why.empty()) return fail(ISP_EINVAL, why);
@@ -620,6 +625,7 @@ int isp_b200_set_kernel_events(isp_b200_pipeline* pl, void* before, void* after)
 int isp_b200_process_host(isp_b200_pipeline* pl, const isp_raw_view_c* raw, const isp_rgb_view_c* out,
                           const isp_stats_c* stats, const isp_exposure_c* exposure) {
   if (pl == nullptr || raw == nullptr || out == nullptr) return fail(ISP_EINVAL, "pipeline, raw or out is null");
+  const TraceRange range("isp.process_host");
   std::string why = validate_raw(*raw, pl->params.c);
   if (why.empty()) why = validate_out(*raw, *out);
   if (!why.empty()) return fail(ISP_EINVAL, why);
@@ -652,8 +658,11 @@ int isp_b200_process_host(isp_b200_pipeline* pl, const isp_raw_view_c* raw, cons
   }
   if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc");
   cudaStream_t s = pl->host_stream;
-  e = cudaMemcpy2DAsync(pl->d_raw, raw_pitch, raw->data, raw->pitch, row, static_cast<size_t>(raw->height),
-                        cudaMemcpyHostToDevice, s);
+  {
+    const TraceRange upload("isp.upload", kTraceCopy);
+    e = cudaMemcpy2DAsync(pl->d_raw, raw_pitch, raw->data, raw->pitch, row, static_cast<size_t>(raw->height),
+                          cudaMemcpyHostToDevice, s);
+  }
   if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy2DAsync");
   isp_raw_view_c draw = *raw;
   draw.data = pl->d_raw;
@@ -665,6 +674,7 @@ int isp_b200_process_host(isp_b200_pipeline* pl, const isp_raw_view_c* raw, cons
                            stats != nullptr && stats->stats != nullptr ? d_st : nullptr};
   const int status = isp_b200_process(pl, &draw, &dout, &dstats, exposure, s);
   if (status != ISP_OK) return status;
+  const TraceRange download("isp.download", kTraceCopy);
   e = cudaMemcpy2DAsync(out->data, out->pitch, pl->d_out, out_row, out_row, static_cast<size_t>(raw->height),
                         cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess && dstats.histogram != nullptr) {

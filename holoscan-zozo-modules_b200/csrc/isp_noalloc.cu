@@ -41,6 +41,7 @@
 #include "isp_b200.h"
 #include "isp_host.hpp"
 #include "isp_kernels.cuh"
+#include "isp_trace.hpp"
 
 namespace isp_b200 {
 namespace {
@@ -183,6 +184,7 @@ extern "C" int isp_b200_process_noalloc(const isp_params_c* params, const isp_ra
                                         const isp_rgb_view_c* out, const isp_stats_c* stats,
                                         const isp_exposure_c* exposure, void* stream_ptr) {
   if (params == nullptr || raw == nullptr || out == nullptr) return fail(ISP_EINVAL, "params, raw or out is null");
+  const TraceRange range("isp.process_noalloc");
   if (const char* why = validate_params(*params)) return fail(ISP_EINVAL, why);
   if (params->tone_curve == ISP_TONE_LUT && params->lut_size > kMaxToneEntries) {
     return fail(ISP_EINVAL, "isp_b200_process_noalloc: a tone table holds at most 4097 entries here");

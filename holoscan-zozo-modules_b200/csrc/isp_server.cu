@@ -43,6 +43,7 @@
 
 #include "isp_b200.h"
 #include "isp_host.hpp"
+#include "isp_trace.hpp"
 
 namespace {
 
@@ -200,6 +201,7 @@ bool reap(isp_b200_server* sv) {
       if (q == cudaErrorNotReady) break;
       if (q != cudaSuccess) worker_fail(sv, "batch", q);
     }
+    const TraceRange range("isp.server.retire", kTraceServe);
     const int64_t t = now_ns();
     for (const InFlight& f : b.frames) {
       Stream& s = *sv->streams[static_cast<size_t>(f.stream)];
@@ -254,6 +256,7 @@ bool admit(isp_b200_server* sv) {
       }
     }
     if (pick < 0) break;
+    const TraceRange range("isp.server.admit", kTraceServe);
     Stream& s = *sv->streams[static_cast<size_t>(pick)];
     DeviceSlot& slot = s.slots[static_cast<size_t>(pick_slot)];
     Admitted a{s.queue.front(), pick_slot, false};
@@ -315,6 +318,7 @@ bool launch_ready(isp_b200_server* sv, std::unique_lock<std::mutex>& lock) {
   ++sv->batches;
   sv->batch_frames += static_cast<int64_t>(batch->frames.size());
   lock.unlock();
+  const TraceRange range("isp.server.launch", kTraceServe);
   // CUDA work outside the lock: submitters only touch the queues, and only
   // the worker touches slots, admitted frames and in-flight batches.
   cudaError_t e = cudaSuccess;

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "isp_host.hpp"
+#include "isp_trace.hpp"
 
 namespace isp_b200 {
 namespace {
@@ -105,6 +106,7 @@ __global__ void __launch_bounds__(256) isp_view_kernel(const __grid_constant__ V
 extern "C" ISP_B200_API int isp_b200_view_compose(const isp_raw_view_c* raw, float black_level, const void* rgb8,
                                                   size_t rgb8_pitch, void* view, size_t view_pitch, void* stream) {
   using namespace isp_b200;
+  const TraceRange range("isp.view", kTraceKernel);
   clear_error();
   if (raw == nullptr || raw->data == nullptr || rgb8 == nullptr || view == nullptr) {
     return fail(ISP_EINVAL, "view_compose: a buffer is missing");
