@@ -1,6 +1,10 @@
 """Builds libisp_b200.so in-tree: the sm_100a kernels and the C ABI.
 
-    python holoscan-zozo-modules_b200/build.py [--verbose]
+    python holoscan-zozo-modules_b200/build.py [--verbose] [--checked]
+
+--checked builds libisp_b200_checked.so instead: the ISP sources compiled with
+ISP_CHECKED, every shared- and global-memory access of the ISP kernels checked
+against the extent of the array it indexes (isp_checked.cuh), for the tests.
 
 Every translation unit is compiled for sm_100a only, without fused
 multiply-add contraction (--fmad=false, -ffp-contract=off): the kernels must
@@ -20,6 +24,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libisp_b200.so")
+OBJ_CHECKED = os.path.join(HERE, "_build_checked")
+LIB_CHECKED = os.path.join(HERE, "libisp_b200_checked.so")
 
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -40,8 +46,8 @@ def _headers(folder: str) -> list:
     return [os.path.join(folder, f) for f in os.listdir(folder) if f.endswith((".cuh", ".hpp"))]
 
 
-def _compile(src: str, verbose: bool) -> str:
-    out = os.path.join(OBJ, os.path.splitext(src)[0].replace("/", "_") + ".o")
+def _compile(src: str, verbose: bool, checked: bool = False) -> str:
+    out = os.path.join(OBJ_CHECKED if checked else OBJ, os.path.splitext(src)[0].replace("/", "_") + ".o")
     path = os.path.join(CSRC, src)
     # A source depends on the headers of its own folder and of csrc/ (the
     # converter's folder includes the ISP's host helpers, not the reverse).
@@ -52,7 +58,9 @@ def _compile(src: str, verbose: bool) -> str:
         deps.append(os.path.join(ROOT, "include", "cc_b200.h"))
     if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
         return out
-    cmd = [NVCC, *ARCH, *COMMON, "-c", path, "-o", out]
+    # The checked build is for tests: its kernels are compiled with less
+    # scheduling effort (the checks make them large), not other arithmetic.
+    cmd = [NVCC, *ARCH, *COMMON, *(["-DISP_CHECKED", "-Xptxas", "-O1"] if checked else []), "-c", path, "-o", out]
     if src.endswith(".cpp"):
         cmd[1:1] = ["-x", "cu"]
     if verbose and src.endswith(".cu"):
@@ -65,21 +73,33 @@ def _compile(src: str, verbose: bool) -> str:
     return out
 
 
-def build(verbose: bool = False) -> str:
-    os.makedirs(OBJ, exist_ok=True)
-    with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as pool:
-        objs = list(pool.map(lambda s: _compile(s, verbose), SOURCES))
+# The checked library holds the ISP alone (not the colour converter).
+CHECKED_SOURCES = [s for s in SOURCES if not s.startswith("cc/")]
+
+
+def _link(lib: str, objs: list) -> None:
     newest = max(os.path.getmtime(o) for o in objs)
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-Xcompiler", "-fPIC"]
+    if not os.path.exists(lib) or os.path.getmtime(lib) < newest:
+        cmd = [NVCC, *ARCH, "-shared", "-o", lib, *objs, "-Xcompiler", "-fPIC"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
-    return LIB
+
+
+def build(verbose: bool = False, checked: bool = False) -> str:
+    """Builds libisp_b200.so (or, with checked, libisp_b200_checked.so)."""
+    os.makedirs(OBJ_CHECKED if checked else OBJ, exist_ok=True)
+    sources = CHECKED_SOURCES if checked else SOURCES
+    with cf.ThreadPoolExecutor(max_workers=len(sources)) as pool:
+        objs = list(pool.map(lambda s: _compile(s, verbose, checked), sources))
+    lib = LIB_CHECKED if checked else LIB
+    _link(lib, objs)
+    return lib
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--checked", action="store_true")
     args = ap.parse_args()
-    print(build(args.verbose))
+    print(build(args.verbose, args.checked))

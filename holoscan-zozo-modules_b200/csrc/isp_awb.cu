@@ -17,9 +17,9 @@ namespace {
 // range and table (the same arithmetic: top + (bottom - top) * ty from
 // T[k] = g + (g' - g) * tx, isp_math.hpp:121-140), for 64 columns and up to
 // kAwbBandRows rows, the rows looped over the block's threads.
-__device__ LscTile build_band_lsc(const FrameDesc& p, const float* grid, int pattern, int x_first, int y_first,
-                                  int nrows, int* col_mx, int* col_ix, float* col_tx, int* row_my, int* row_k,
-                                  float* row_ty, float* table, int* minmax) {
+__device__ LscTile build_band_lsc(const FrameDesc& p, Span<const float> grid, int pattern, int x_first, int y_first,
+                                  int nrows, Span<int> col_mx, Span<int> col_ix, Span<float> col_tx, Span<int> row_my, Span<int> row_k,
+                                  Span<float> row_ty, Span<float> table, int* minmax) {
   constexpr int kCols = 64;
   const int t = threadIdx.x;
   if (t == 0) {
@@ -75,7 +75,7 @@ __device__ LscTile build_band_lsc(const FrameDesc& p, const float* grid, int pat
     const int par = kp % planes;
     const int k = kp / planes;
     const int ch = step == 4 ? cfa_of(pattern, (par << 1) | (col_mx[i] & 1)) : 0;
-    const float* g = grid + ((lt.iy0 + k) * p.lsc_width + col_ix[i]) * step + ch;
+    Span<const float> g = grid + ((lt.iy0 + k) * p.lsc_width + col_ix[i]) * step + ch;
     table[(k * 2 + par) * kSW + i] = g[0] + (g[step] - g[0]) * col_tx[i];
   }
   for (int j = t; j < nrows; j += kThreads) row_k[j] -= lt.iy0;
@@ -93,22 +93,28 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_kernel(const __grid_const
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
   constexpr int kBoxRows = 64;
-  uint8_t* boxes = smem;                                                  // [2][64][128]: double buffer
-  float* table = reinterpret_cast<float*>(smem + 2 * 64 * 128);           // [kLscTableRows][2][kSW]
-  int* col_mx = reinterpret_cast<int*>(table + kLscTableRows * 2 * kSW);  // [64] x 3
-  int* col_ix = col_mx + 64;
-  float* col_tx = reinterpret_cast<float*>(col_ix + 64);
-  int* row_my = reinterpret_cast<int*>(col_tx + 64);                      // [kAwbBandRows] x 3
-  int* row_k = row_my + kAwbBandRows;
-  float* row_ty = reinterpret_cast<float*>(row_k + kAwbBandRows);
-  unsigned int* hist = reinterpret_cast<unsigned int*>(row_ty + kAwbBandRows);  // [3][1024]
-  float* grid_s = reinterpret_cast<float*>(hist + 3 * kAwbBins);          // [kGridSmemGains]
+  constexpr int kTableAt = 2 * 64 * 128;                          // boxes: [2][64][128], a double buffer
+  constexpr int kColsAt = kTableAt + kLscTableRows * 2 * kSW * 4;  // table: [kLscTableRows][2][kSW]
+  constexpr int kRowsAt = kColsAt + 3 * 64 * 4;                    // col_mx, col_ix, col_tx: [64] each
+  constexpr int kHistAt = kRowsAt + 3 * kAwbBandRows * 4;          // row_my, row_k, row_ty: [kAwbBandRows] each
+  constexpr int kGridAt = kHistAt + 3 * kAwbBins * 4;              // hist: [3][1024]; grid_s: [kGridSmemGains]
+  CheckRecord* rec = span_rec(p.scratch);
+  Span<uint8_t> boxes = carve_span<uint8_t>(smem, 0, kTableAt, rec);
+  Span<float> table = carve_span<float>(smem, kTableAt, kColsAt - kTableAt, rec);
+  Span<int> col_mx = carve_span<int>(smem, kColsAt, 64 * 4, rec);
+  Span<int> col_ix = carve_span<int>(smem, kColsAt + 64 * 4, 64 * 4, rec);
+  Span<float> col_tx = carve_span<float>(smem, kColsAt + 128 * 4, 64 * 4, rec);
+  Span<int> row_my = carve_span<int>(smem, kRowsAt, kAwbBandRows * 4, rec);
+  Span<int> row_k = carve_span<int>(smem, kRowsAt + kAwbBandRows * 4, kAwbBandRows * 4, rec);
+  Span<float> row_ty = carve_span<float>(smem, kRowsAt + 2 * kAwbBandRows * 4, kAwbBandRows * 4, rec);
+  Span<unsigned int> hist = carve_span<unsigned int>(smem, kHistAt, kGridAt - kHistAt, rec);
+  Span<float> grid_s = carve_span<float>(smem, kGridAt, kGridSmemGains * 4, rec);
   __shared__ uint64_t bars[2];
   __shared__ u64 red[kWarps];
   __shared__ int minmax[2];
   __shared__ int first;
   __shared__ bool last;
-  Scratch* s = p.scratch;
+  Span<Scratch> s = p.scratch;
   const int tid = threadIdx.x;
   const int box_bytes = awb_box_bytes(p.raw_format);
   // The tile pass that follows may launch now: it waits (griddepcontrol.wait)
@@ -119,7 +125,7 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_kernel(const __grid_const
     for (int i = tid; i < 3 * kAwbBins; i += kThreads) hist[i] = 0U;
   }
   // The lens shading gains in shared memory for the frame, when they fit.
-  const float* grid = p.lsc;
+  Span<const float> grid = p.lsc;
   const int gains = p.lsc_width * p.lsc_height * p.lsc_channels;
   if (p.lsc != nullptr && gains <= kGridSmemGains) {
     for (int i = tid; i < gains; i += kThreads) cp_async4(&grid_s[i], &p.lsc[i]);
@@ -164,7 +170,7 @@ __global__ void __launch_bounds__(kThreads, 3) isp_awb_kernel(const __grid_const
       if (tid == 0) report_wait_timeout(s);
     }
     phases ^= 1U << buf;
-    const uint8_t* box = boxes + buf * 64 * 128;
+    Span<const uint8_t> box = boxes + buf * 64 * 128;
     const int rows = (ty - ty0) * 64;  // the tile's first row within the band
     unsigned int sum[3] = {0U, 0U, 0U};
     unsigned int quads = 0;

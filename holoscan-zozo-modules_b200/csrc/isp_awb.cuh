@@ -24,10 +24,10 @@ __device__ __forceinline__ int awb_box_x(int fmt, int x0) {
 // per-tile sums (at most 8 samples of 2^22 per colour and thread) and, for
 // white patch, the block's bins.
 template <int kFmt, int kSrc, bool kWhitePatch, int kPat>
-__device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box, int box_bytes, int x0, int y0,
-                                         const LscTile& lt, const int* row_k, const float* row_ty,
-                                         const float* table, const float (&black)[4], const float (&inv)[4],
-                                         unsigned int* hist, unsigned int (&sum)[3], unsigned int& quads) {
+__device__ __forceinline__ void awb_tile(const FrameDesc& p, Span<const uint8_t> box, int box_bytes, int x0, int y0,
+                                         const LscTile& lt, Span<const int> row_k, Span<const float> row_ty,
+                                         Span<const float> table, const float (&black)[4], const float (&inv)[4],
+                                         Span<unsigned int> hist, unsigned int (&sum)[3], unsigned int& quads) {
   const int quads_x = p.width / 2;
   const int quads_y = p.height / 2;
   const unsigned int white = static_cast<unsigned int>(p.white);
@@ -43,19 +43,19 @@ __device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box,
     if (qy >= quads_y || qx0 >= quads_x) continue;
     unsigned int top[4], bot[4];
     if constexpr (kSrc == 0) {
-      const uint8_t* r0 = box + (2 * a) * box_bytes;
-      const uint8_t* r1 = r0 + box_bytes;
+      Span<const uint8_t> r0 = box + (2 * a) * box_bytes;
+      Span<const uint8_t> r1 = r0 + box_bytes;
       if constexpr (kFmt == kRawU8) {
-        const unsigned int w0 = *reinterpret_cast<const unsigned int*>(r0 + 4 * u);
-        const unsigned int w1 = *reinterpret_cast<const unsigned int*>(r1 + 4 * u);
+        const unsigned int w0 = *span_cast<const unsigned int>(r0 + 4 * u);
+        const unsigned int w1 = *span_cast<const unsigned int>(r1 + 4 * u);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           top[k] = (w0 >> (8 * k)) & 0xFFU;
           bot[k] = (w1 >> (8 * k)) & 0xFFU;
         }
       } else if constexpr (kFmt == kRawU16) {
-        const uint2 w0 = *reinterpret_cast<const uint2*>(r0 + 8 * u);
-        const uint2 w1 = *reinterpret_cast<const uint2*>(r1 + 8 * u);
+        const uint2 w0 = *span_cast<const uint2>(r0 + 8 * u);
+        const uint2 w1 = *span_cast<const uint2>(r1 + 8 * u);
         top[0] = w0.x & 0xFFFFU; top[1] = w0.x >> 16; top[2] = w0.y & 0xFFFFU; top[3] = w0.y >> 16;
         bot[0] = w1.x & 0xFFFFU; bot[1] = w1.x >> 16; bot[2] = w1.y & 0xFFFFU; bot[3] = w1.y >> 16;
       } else {
@@ -98,8 +98,8 @@ __device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box,
           const int kk = row_k[rj];
           const float2 tyj = bc2(row_ty[rj]);
           const int pl = p.lsc_channels == 4 ? r : 0;
-          const float4 t0 = *reinterpret_cast<const float4*>(table + (kk * 2 + pl) * kSW + 4 * u);
-          const float4 t1 = *reinterpret_cast<const float4*>(table + ((kk + 1) * 2 + pl) * kSW + 4 * u);
+          const float4 t0 = *span_cast<const float4>(table + (kk * 2 + pl) * kSW + 4 * u);
+          const float4 t1 = *span_cast<const float4>(table + ((kk + 1) * 2 + pl) * kSW + 4 * u);
           // gain = t0 + (t1 - t0) ty per column (lens_shading_gain, isp_math.hpp:121-140).
           const float2 a0 = make_float2(t0.x, t0.z), a1 = make_float2(t0.y, t0.w);
           const float2 g0 = add_lanes(a0, mul2(sub2(make_float2(t1.x, t1.z), a0), tyj));
@@ -134,7 +134,7 @@ __device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box,
         // trunc(x 1024): an exact product, so its two-lane truncation is safe.
         const float2 b = magic_trunc2(mul2(x, bc2(static_cast<float>(kAwbBins))));
         const unsigned int b0 = magic_int(b.x), b1 = magic_int(b.y);
-        unsigned int* h = hist + color_of(cfa_of(kPat, k)) * kAwbBins;
+        Span<unsigned int> h = hist + color_of(cfa_of(kPat, k)) * kAwbBins;
         if (ok0) atomicAdd(&h[b0 < kAwbBins - 1 ? b0 : kAwbBins - 1], 1U);
         if (ok1) atomicAdd(&h[b1 < kAwbBins - 1 ? b1 : kAwbBins - 1], 1U);
       }
@@ -150,10 +150,10 @@ __device__ __forceinline__ void awb_tile(const FrameDesc& p, const uint8_t* box,
 }
 
 template <int kSrc, bool kWhitePatch, int kPat>
-__device__ __forceinline__ void awb_tile_fmt(const FrameDesc& p, const uint8_t* box, int box_bytes, int x0, int y0,
-                                             const LscTile& lt, const int* row_k, const float* row_ty,
-                                             const float* table, const float (&black)[4], const float (&inv)[4],
-                                             unsigned int* hist, unsigned int (&sum)[3], unsigned int& quads) {
+__device__ __forceinline__ void awb_tile_fmt(const FrameDesc& p, Span<const uint8_t> box, int box_bytes, int x0, int y0,
+                                             const LscTile& lt, Span<const int> row_k, Span<const float> row_ty,
+                                             Span<const float> table, const float (&black)[4], const float (&inv)[4],
+                                             Span<unsigned int> hist, unsigned int (&sum)[3], unsigned int& quads) {
   if constexpr (kSrc == 1) {
     awb_tile<kRawU8, 1, kWhitePatch, kPat>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads);
   } else {
@@ -184,9 +184,9 @@ __device__ __forceinline__ void awb_tile_fmt(const FrameDesc& p, const uint8_t* 
 // (which reads and writes the white balance state that tile pass read) must
 // follow it.
 template <bool kAfterPrevious = false>
-__device__ void awb_flush(const FrameDesc& p, const u64 (&acc)[4], const unsigned int* hist, bool white_patch,
+__device__ void awb_flush(const FrameDesc& p, const u64 (&acc)[4], Span<const unsigned int> hist, bool white_patch,
                           u64* red, int* first, bool* last, unsigned int tiles_done, unsigned int tiles_total) {
-  Scratch* s = p.scratch;
+  Span<Scratch> s = p.scratch;
   const int tid = threadIdx.x;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -195,8 +195,9 @@ __device__ void awb_flush(const FrameDesc& p, const u64 (&acc)[4], const unsigne
   }
   if (white_patch) {
     __syncthreads();
+    const Span<unsigned int> bins = sub_span(s, &s->awb_hist[0][0], 3 * kAwbBins);
     for (int i = tid; i < 3 * kAwbBins; i += kThreads) {
-      if (hist[i] != 0U) atomicAdd(&s->awb_hist[0][0] + i, hist[i]);
+      if (hist[i] != 0U) atomicAdd(&bins[i], hist[i]);
     }
   }
   __threadfence();

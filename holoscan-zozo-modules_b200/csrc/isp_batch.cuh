@@ -34,7 +34,7 @@ __device__ __forceinline__ void load_desc(FrameDesc* dst, const FrameDesc* src) 
 }
 
 // The frame holding work item `item`, searching forward from frame `from`.
-__device__ __forceinline__ int frame_of_item(const BatchFrame* frames, int nframes, int from, int item, bool awb) {
+__device__ __forceinline__ int frame_of_item(Span<const BatchFrame> frames, int nframes, int from, int item, bool awb) {
   int f = from;
   while (f + 1 < nframes && item >= (awb ? frames[f + 1].awb_begin : frames[f + 1].tile_begin)) ++f;
   return f;
@@ -42,12 +42,19 @@ __device__ __forceinline__ int frame_of_item(const BatchFrame* frames, int nfram
 
 template <bool kLutSmem, int kTileH>
 __global__ void __launch_bounds__(kThreads, kTileH == kTH ? 2 : 3)
-    isp_batch_kernel(const BatchFrame* frames, int nframes, const int2* ranges) {
+    isp_batch_kernel(const BatchFrame* frames_in, int nframes, const int2* ranges_in) {
   using GS = Geom<true, kTileH>;  // the sharpening geometry holds every variant's
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
+#ifdef ISP_CHECKED
+  CheckRecord* const rec = span_rec(frames_in[0].desc.scratch);
+#else
+  CheckRecord* const rec = nullptr;
+#endif
+  const Span<const BatchFrame> frames = make_span(frames_in, static_cast<size_t>(nframes), rec);
+  const Span<const int2> ranges = make_span(ranges_in, static_cast<size_t>(gridDim.x), rec);
   const TileSmem m =
-      carve(smem, layout_of(true, box_row_bytes(kRawU16), kLutSmem ? kBatchLutEntries : 0, kTileH), GS::kSH);
+      carve(smem, layout_of(true, box_row_bytes(kRawU16), kLutSmem ? kBatchLutEntries : 0, kTileH), GS::kSH, rec);
   __shared__ uint64_t bar;
   __shared__ u64 red[4 * kWarps];
   __shared__ int minmax[2];
@@ -125,10 +132,10 @@ __global__ void __launch_bounds__(kThreads, kTileH == kTH ? 2 : 3)
 
 // The statistics tile of a frame for its Bayer pattern and mode.
 template <int kSrc>
-__device__ __forceinline__ void awb_tile_any(const FrameDesc& p, int pattern, bool white_patch, const uint8_t* box,
-                                             int box_bytes, int x0, int y0, const LscTile& lt, const int* row_k,
-                                             const float* row_ty, const float* table, const float (&black)[4],
-                                             const float (&inv)[4], unsigned int* hist, unsigned int (&sum)[3],
+__device__ __forceinline__ void awb_tile_any(const FrameDesc& p, int pattern, bool white_patch, Span<const uint8_t> box,
+                                             int box_bytes, int x0, int y0, const LscTile& lt, Span<const int> row_k,
+                                             Span<const float> row_ty, Span<const float> table, const float (&black)[4],
+                                             const float (&inv)[4], Span<unsigned int> hist, unsigned int (&sum)[3],
                                              unsigned int& quads) {
 #define ISP_AWB_CASE(P, W) \
   awb_tile_fmt<kSrc, W, P>(p, box, box_bytes, x0, y0, lt, row_k, row_ty, table, black, inv, hist, sum, quads)
@@ -145,19 +152,30 @@ __device__ __forceinline__ void awb_tile_any(const FrameDesc& p, int pattern, bo
 #undef ISP_AWB_CASE
 }
 
-__global__ void __launch_bounds__(kThreads, 3) isp_awb_batch_kernel(const BatchFrame* frames, int nframes,
-                                                               const int2* ranges) {
+__global__ void __launch_bounds__(kThreads, 3) isp_awb_batch_kernel(const BatchFrame* frames_in, int nframes,
+                                                               const int2* ranges_in) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
-  uint8_t* boxes = smem;                                                  // [2][64][128]: double buffer
-  float* table = reinterpret_cast<float*>(smem + 2 * 64 * 128);           // [kLscTableRows][2][kSW]
-  int* col_mx = reinterpret_cast<int*>(table + kLscTableRows * 2 * kSW);  // [64] x 3
-  int* col_ix = col_mx + 64;
-  float* col_tx = reinterpret_cast<float*>(col_ix + 64);
-  int* row_my = reinterpret_cast<int*>(col_tx + 64);                      // [64] x 3
-  int* row_k = row_my + 64;
-  float* row_ty = reinterpret_cast<float*>(row_k + 64);
-  unsigned int* hist = reinterpret_cast<unsigned int*>(row_ty + 64);      // [3][1024]
+#ifdef ISP_CHECKED
+  CheckRecord* const rec = span_rec(frames_in[0].desc.scratch);
+#else
+  CheckRecord* const rec = nullptr;
+#endif
+  const Span<const BatchFrame> frames = make_span(frames_in, static_cast<size_t>(nframes), rec);
+  const Span<const int2> ranges = make_span(ranges_in, static_cast<size_t>(gridDim.x), rec);
+  constexpr int kTableAt = 2 * 64 * 128;                          // boxes: [2][64][128], a double buffer
+  constexpr int kColsAt = kTableAt + kLscTableRows * 2 * kSW * 4;  // table: [kLscTableRows][2][kSW]
+  constexpr int kRowsAt = kColsAt + 3 * 64 * 4;                    // col_mx, col_ix, col_tx: [64] each
+  constexpr int kHistAt = kRowsAt + 3 * 64 * 4;                    // row_my, row_k, row_ty: [64] each
+  Span<uint8_t> boxes = carve_span<uint8_t>(smem, 0, kTableAt, rec);
+  Span<float> table = carve_span<float>(smem, kTableAt, kColsAt - kTableAt, rec);
+  Span<int> col_mx = carve_span<int>(smem, kColsAt, 64 * 4, rec);
+  Span<int> col_ix = carve_span<int>(smem, kColsAt + 64 * 4, 64 * 4, rec);
+  Span<float> col_tx = carve_span<float>(smem, kColsAt + 128 * 4, 64 * 4, rec);
+  Span<int> row_my = carve_span<int>(smem, kRowsAt, 64 * 4, rec);
+  Span<int> row_k = carve_span<int>(smem, kRowsAt + 64 * 4, 64 * 4, rec);
+  Span<float> row_ty = carve_span<float>(smem, kRowsAt + 128 * 4, 64 * 4, rec);
+  Span<unsigned int> hist = carve_span<unsigned int>(smem, kHistAt, 3 * kAwbBins * 4, rec);  // [3][1024]
   __shared__ uint64_t bars[2];
   __shared__ u64 red[4 * kWarps];
   __shared__ int minmax[2];

@@ -136,9 +136,20 @@ cudaError_t device_state_reset_awb(const isp_params_c& p, DeviceState* s, cudaSt
 FrameDesc make_desc(const isp_params_c& p, const DeviceState& s, const isp_raw_view_c& raw,
                     const isp_rgb_view_c& out, const isp_stats_c* stats, const isp_exposure_c* exposure) {
   FrameDesc d{};
+  // Each buffer's extent, which the bounds-checked build holds its accesses
+  // to (the regular build keeps plain pointers).
+#ifdef ISP_CHECKED
+  CheckRecord* rec = &s.scratch->check;
+#else
+  CheckRecord* rec = nullptr;
+#endif
+  const size_t rows_before_last = static_cast<size_t>(raw.height - 1);
+  const size_t out_row = static_cast<size_t>(raw.width) * (out.format == ISP_OUT_RGBA8 ? 4U : 3U) *
+                         (out.format == ISP_OUT_RGB16 ? 2U : out.format == ISP_OUT_RGB32F ? 4U : 1U);
   d.width = raw.width;
   d.height = raw.height;
-  d.raw = static_cast<const uint8_t*>(raw.data);
+  d.raw = make_span(static_cast<const uint8_t*>(raw.data),
+                    raw.pitch * rows_before_last + raw_row_bytes(raw.format, raw.width), rec);
   d.raw_pitch = static_cast<int64_t>(raw.pitch);
   d.raw_format = raw.format;
   d.pattern = raw.pattern;
@@ -152,7 +163,8 @@ FrameDesc make_desc(const isp_params_c& p, const DeviceState& s, const isp_raw_v
   for (int k = 0; k < 3; ++k) d.wb[k] = p.wb_gains[k];
   d.auto_wb = p.white_balance != ISP_WB_MANUAL;
   if (p.has_lens_shading) {
-    d.lsc = s.lsc;
+    d.lsc = make_span(static_cast<const float*>(s.lsc),
+                      static_cast<size_t>(p.lsc_width) * p.lsc_height * p.lsc_channels, rec);
     d.lsc_width = p.lsc_width;
     d.lsc_height = p.lsc_height;
     d.lsc_channels = p.lsc_channels;
@@ -160,17 +172,18 @@ FrameDesc make_desc(const isp_params_c& p, const DeviceState& s, const isp_raw_v
     d.lsc_sy = static_cast<float>(p.lsc_height - 1) / static_cast<float>(raw.height - 1);
   }
   for (int k = 0; k < 9; ++k) d.ccm[k] = p.ccm[k];
-  d.tone = s.tone;
+  d.tone = make_span(static_cast<const float2*>(s.tone), static_cast<size_t>(s.tone_size), rec);
   d.tone_size = s.tone_size;
   d.tone_last = s.tone_last;
   d.sharpen = p.sharpen;
-  d.out = static_cast<uint8_t*>(out.data);
+  d.out = make_span(static_cast<uint8_t*>(out.data), out.pitch * rows_before_last + out_row, rec);
   d.out_pitch = static_cast<int64_t>(out.pitch);
   d.out_format = out.format;
   d.out_vector = (reinterpret_cast<uintptr_t>(out.data) % 16U == 0U) && (out.pitch % 16U == 0U);
-  d.hist_out = stats != nullptr ? stats->histogram : nullptr;
-  d.stats_out = stats != nullptr ? stats->stats : nullptr;
-  d.scratch = s.scratch;
+  d.hist_out = make_span(stats != nullptr ? stats->histogram : nullptr,
+                         static_cast<size_t>(ISP_HISTOGRAM_CHANNELS) * ISP_HISTOGRAM_BINS, rec);
+  d.stats_out = make_span(stats != nullptr ? stats->stats : nullptr, static_cast<size_t>(ISP_STATS_SIZE), rec);
+  d.scratch = make_span(s.scratch, 1, rec);
   d.ae.target = p.auto_exposure.target;
   d.ae.damping = p.auto_exposure.damping;
   d.ae.min_exposure_ns = p.auto_exposure.min_exposure_ns;
@@ -216,7 +229,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 bool encode_raw_map(const FrameDesc& d, int box_row_bytes, int box_rows, CUtensorMap* map) {
   std::memset(map, 0, sizeof(*map));
-  const auto base = reinterpret_cast<uintptr_t>(d.raw);
+  const auto base = reinterpret_cast<uintptr_t>(span_ptr(d.raw));
   if (base % 16U != 0U || d.raw_pitch % 16 != 0 || d.raw_pitch >= (int64_t{1} << 40)) return false;
   PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
   if (encode == nullptr) return false;
@@ -228,7 +241,7 @@ bool encode_raw_map(const FrameDesc& d, int box_row_bytes, int box_rows, CUtenso
                              static_cast<cuuint32_t>(box_rows)};
   const cuuint32_t elem[2] = {1, 1};
   const CUresult r = encode(map, u16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
-                            const_cast<uint8_t*>(d.raw), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            const_cast<uint8_t*>(span_ptr(d.raw)), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
@@ -591,6 +604,33 @@ int isp_b200_device_status(isp_b200_pipeline* pl, int32_t* status) {
   *status = value;
   clear_error();
   return ISP_OK;
+}
+
+int isp_b200_checked_violations(isp_b200_pipeline* pl, uint32_t* count, uint64_t* first_address) {
+  if (pl == nullptr || count == nullptr || first_address == nullptr) {
+    return fail(ISP_EINVAL, "pipeline, count or first_address is null");
+  }
+#ifdef ISP_CHECKED
+  if (pl->queued) {
+    const cudaError_t e = cudaEventSynchronize(pl->done);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaEventSynchronize");
+  }
+  CheckRecord record{};
+  const CheckRecord zero{};
+  PrivateStream ps;
+  ps.copy(&record, &pl->state.scratch->check, sizeof(CheckRecord), cudaMemcpyDeviceToHost);
+  ps.copy(&pl->state.scratch->check, &zero, sizeof(CheckRecord), cudaMemcpyHostToDevice);
+  const cudaError_t e = ps.finish();
+  if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyAsync");
+  *count = record.count;
+  *first_address = record.count != 0U ? record.address : 0U;
+  clear_error();
+  return ISP_OK;
+#else
+  *count = 0;
+  *first_address = 0;
+  return fail(ISP_EINVAL, "isp_b200_checked_violations: this is not the bounds-checked build (libisp_b200_checked.so)");
+#endif
 }
 
 int isp_b200_check_bounded_wait(isp_b200_pipeline* pl, uint32_t polls, void* stream_ptr) {

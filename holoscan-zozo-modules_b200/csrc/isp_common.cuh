@@ -152,13 +152,22 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, void* dst, uint64_t* bar, int x, int y,
+// Requests a box of `bytes` bytes into dst, completing on bar. (The checked
+// build makes no copy whose box would leave dst's region: it arrives on the
+// barrier without one, so that the wait still ends.)
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, Span<uint8_t> dst, uint64_t* bar, int x, int y,
                                             unsigned int bytes) {
+#ifdef ISP_CHECKED
+  if (span_range(dst, bytes) != span_ptr(dst)) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+    return;
+  }
+#endif
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-      "[%4];" ::"r"(smem_u32(dst)),
+      "[%4];" ::"r"(smem_u32(span_ptr(dst))),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
@@ -179,7 +188,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
 
 // A bounded wait gave up: the frame's outputs are not trustworthy. The flag
 // stays set until isp_b200_device_status reads and clears it.
-__device__ __forceinline__ void report_wait_timeout(Scratch* s) { atomicExch(&s->error, 1); }
+__device__ __forceinline__ void report_wait_timeout(Span<Scratch> s) { atomicExch(&s->error, 1); }
 
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
@@ -188,10 +197,22 @@ __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy
 // plain loads and stores waits out one L2 round trip per iteration), and
 // cp_async_wait_all() returns once this thread's copies have landed.
 __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+#ifdef ISP_CHECKED
+  if (!__isShared(dst)) {  // a refused destination: the check's sink in global memory
+    *static_cast<uint32_t*>(dst) = *static_cast<const uint32_t*>(src);
+    return;
+  }
+#endif
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src))
                : "memory");
 }
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+#ifdef ISP_CHECKED
+  if (!__isShared(dst)) {
+    *static_cast<uint2*>(dst) = *static_cast<const uint2*>(src);
+    return;
+  }
+#endif
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src))
                : "memory");
 }
@@ -206,13 +227,13 @@ __device__ __forceinline__ int box_x(int fmt, int x0) {
 // ---- Raw unpacking from a box row ----------------------------------------
 
 // Samples x0 - 4 + 4u .. + 3 of a box row (box starting at box_x(fmt, x0)).
-__device__ __forceinline__ void unpack4(int fmt, const uint8_t* row, int u, unsigned int s[4]) {
+__device__ __forceinline__ void unpack4(int fmt, Span<const uint8_t> row, int u, unsigned int s[4]) {
   if (fmt == kRawU8) {
-    const unsigned int w = *reinterpret_cast<const unsigned int*>(row + 12 + 4 * u);
+    const unsigned int w = *span_cast<const unsigned int>(row + 12 + 4 * u);
 #pragma unroll
     for (int k = 0; k < 4; ++k) s[k] = (w >> (8 * k)) & 0xFFU;
   } else if (fmt == kRawU16) {
-    const uint2 w = *reinterpret_cast<const uint2*>(row + 8 + 8 * u);
+    const uint2 w = *span_cast<const uint2>(row + 8 + 8 * u);
     s[0] = w.x & 0xFFFFU;
     s[1] = w.x >> 16;
     s[2] = w.y & 0xFFFFU;
@@ -220,7 +241,7 @@ __device__ __forceinline__ void unpack4(int fmt, const uint8_t* row, int u, unsi
   } else if (fmt == kRawRaw10) {
     // Group g0 - 1 + u at byte 11 + 5u: four high bytes, then the low bits.
     const int b = 11 + 5 * u;
-    const unsigned int* w = reinterpret_cast<const unsigned int*>(row + (b & ~3));
+    Span<const unsigned int> w = span_cast<const unsigned int>(row + (b & ~3));
     const unsigned int sh = 8U * static_cast<unsigned int>(b & 3);
     const unsigned int hi4 = __funnelshift_r(w[0], w[1], sh);
     const unsigned int lo = (w[1] >> sh) & 0xFFU;
@@ -229,7 +250,7 @@ __device__ __forceinline__ void unpack4(int fmt, const uint8_t* row, int u, unsi
   } else {
     // Two groups of three bytes at byte 10 + 6u.
     const int b = 10 + 6 * u;
-    const unsigned int* w = reinterpret_cast<const unsigned int*>(row + (b & ~3));
+    Span<const unsigned int> w = span_cast<const unsigned int>(row + (b & ~3));
     const unsigned int sh = 8U * static_cast<unsigned int>(b & 3);
     const unsigned int v0 = __funnelshift_r(w[0], w[1], sh);  // a0 a1 a2 b0
     const unsigned int v1 = w[1] >> sh;                        // b1 b2 ..
@@ -243,15 +264,15 @@ __device__ __forceinline__ void unpack4(int fmt, const uint8_t* row, int u, unsi
 }
 
 // One sample at image column mx of a box row (box starting at box_x(fmt, x0)).
-__device__ __forceinline__ unsigned int unpack1(int fmt, const uint8_t* row, int mx, int x0) {
+__device__ __forceinline__ unsigned int unpack1(int fmt, Span<const uint8_t> row, int mx, int x0) {
   if (fmt == kRawU8) return row[mx - x0 + 16];
-  if (fmt == kRawU16) return *reinterpret_cast<const uint16_t*>(row + 2 * (mx - x0 + 8));
+  if (fmt == kRawU16) return *span_cast<const uint16_t>(row + 2 * (mx - x0 + 8));
   if (fmt == kRawRaw10) {
-    const uint8_t* g = row + 5 * ((mx >> 2) - (x0 >> 2)) + 16;
+    Span<const uint8_t> g = row + 5 * ((mx >> 2) - (x0 >> 2)) + 16;
     const int k = mx & 3;
     return (static_cast<unsigned int>(g[k]) << 2) | ((g[4] >> (2 * k)) & 3U);
   }
-  const uint8_t* g = row + 3 * ((mx >> 1) - (x0 >> 1)) + 16;
+  Span<const uint8_t> g = row + 3 * ((mx >> 1) - (x0 >> 1)) + 16;
   const int k = mx & 1;
   return (static_cast<unsigned int>(g[k]) << 4) | ((g[2] >> (4 * k)) & 15U);
 }
@@ -276,10 +297,10 @@ struct LscTile {
 // `grid`: the frame's lens shading gains (the frame's own, or a copy in
 // shared memory).
 template <bool kPaired = false>
-__device__ LscTile build_lsc(const FrameDesc& p, const float* grid, int pattern, int x_first, int ncols, int y_first,
+__device__ LscTile build_lsc(const FrameDesc& p, Span<const float> grid, int pattern, int x_first, int ncols, int y_first,
                              int nrows,
-                             bool mirror_xy, int xclamp, int yclamp, int* col_mx, int* col_ix, float* col_tx,
-                             int* row_my, int* row_k, float* row_ty, float* table, int* minmax) {
+                             bool mirror_xy, int xclamp, int yclamp, Span<int> col_mx, Span<int> col_ix, Span<float> col_tx,
+                             Span<int> row_my, Span<int> row_k, Span<float> row_ty, Span<float> table, int* minmax) {
   const int t = threadIdx.x;
   if (t == 0) {
     minmax[0] = 0x7FFFFFFF;
@@ -334,11 +355,11 @@ __device__ LscTile build_lsc(const FrameDesc& p, const float* grid, int pattern,
   const int planes = step == 4 ? 2 : 1;
   const auto entry = [&](int k, int par, int i) {
     const int ch = step == 4 ? cfa_of(pattern, (par << 1) | (col_mx[i] & 1)) : 0;
-    const float* g = grid + ((lt.iy0 + k) * p.lsc_width + col_ix[i]) * step + ch;
+    Span<const float> g = grid + ((lt.iy0 + k) * p.lsc_width + col_ix[i]) * step + ch;
     return g[0] + (g[step] - g[0]) * col_tx[i];
   };
   if constexpr (kPaired) {
-    float2* table2 = reinterpret_cast<float2*>(table);
+    Span<float2> table2 = span_cast<float2>(table);
     for (int e = t; e < lt.rows * planes * kPW; e += kThreads) {
       const int i = e % kPW;
       const int kp = e / kPW;
@@ -368,9 +389,9 @@ __device__ LscTile build_lsc(const FrameDesc& p, const float* grid, int pattern,
 // Tiles whose table would not fit take build_lsc<true>. Of the column maps
 // only the columns themselves are written (the path of phase A without a TMA
 // box reads them); the cells are worked out where the table needs them.
-__device__ LscTile build_lsc_inner(const FrameDesc& p, const float* grid, int pattern, int x_first, int y_first,
-                                   int nrows, int* col_mx, int* col_ix, float* col_tx, int* row_my, int* row_k,
-                                   float* row_ty, float* table, int* minmax) {
+__device__ LscTile build_lsc_inner(const FrameDesc& p, Span<const float> grid, int pattern, int x_first, int y_first,
+                                   int nrows, Span<int> col_mx, Span<int> col_ix, Span<float> col_tx, Span<int> row_my, Span<int> row_k,
+                                   Span<float> row_ty, Span<float> table, int* minmax) {
   LscTile lt{0, 0};
   const int t = threadIdx.x;
   if (p.lsc == nullptr) {
@@ -408,10 +429,10 @@ __device__ LscTile build_lsc_inner(const FrameDesc& p, const float* grid, int pa
     ix = ix > p.lsc_width - 2 ? p.lsc_width - 2 : ix;
     const float tx = fx - static_cast<float>(ix);
     const int ch = step == 4 ? cfa_of(pattern, (par << 1) | (x & 1)) : 0;
-    const float* g = grid + ((lt.iy0 + k) * p.lsc_width + ix) * step + ch;
+    Span<const float> g = grid + ((lt.iy0 + k) * p.lsc_width + ix) * step + ch;
     return g[0] + (g[step] - g[0]) * tx;
   };
-  float2* table2 = reinterpret_cast<float2*>(table);
+  Span<float2> table2 = span_cast<float2>(table);
   for (int e = t; e < lt.rows * planes * kPW; e += kThreads) {
     const int i = e % kPW;
     const int kp = e / kPW;
@@ -482,13 +503,13 @@ __device__ u64 block_exclusive_scan(u64 v, u64* red) {
 // histogram_percentile (isp_math.hpp:336-352) by the whole block: thread t
 // owns bins 4t..4t+3; the prefix counts are exact integers, so every
 // comparison is the reference's.
-__device__ float block_percentile(const unsigned int* hist, float percentile, u64* red, int* first) {
+__device__ float block_percentile(Span<const unsigned int> hist, float percentile, u64* red, int* first) {
   const int t = threadIdx.x;
   unsigned int h[4];
   u64 mine = 0;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    h[k] = __ldcg(hist + 4 * t + k);
+    h[k] = __ldcg(&hist[4 * t + k]);
     mine += h[k];
   }
   const u64 total = block_sum(mine, red);
@@ -528,7 +549,7 @@ __device__ float block_percentile(const unsigned int* hist, float percentile, u6
 
 // finish_white_balance (isp_math.hpp:357-384) in the statistics pass's last
 // CTA; then the sums are cleared for the next frame.
-__device__ void awb_finish(const FrameDesc& p, Scratch* s, u64* red, int* first) {
+__device__ void awb_finish(const FrameDesc& p, Span<Scratch> s, u64* red, int* first) {
   const u64 nquads = __ldcg(&s->awb_quads);
   float level[3] = {0.0F, 0.0F, 0.0F};
   if (nquads != 0) {
@@ -538,7 +559,7 @@ __device__ void awb_finish(const FrameDesc& p, Scratch* s, u64* red, int* first)
       level[1] = static_cast<float>(static_cast<double>(__ldcg(&s->awb_sum[1])) / (2.0 * q));
       level[2] = static_cast<float>(static_cast<double>(__ldcg(&s->awb_sum[2])) / q);
     } else {
-      for (int k = 0; k < 3; ++k) level[k] = block_percentile(s->awb_hist[k], p.awb_percentile, red, first);
+      for (int k = 0; k < 3; ++k) level[k] = block_percentile(sub_span(s, &s->awb_hist[k][0], kAwbBins), p.awb_percentile, red, first);
     }
   }
   __syncthreads();
@@ -553,7 +574,8 @@ __device__ void awb_finish(const FrameDesc& p, Scratch* s, u64* red, int* first)
     }
     s->awb_valid = 1;
   }
-  for (int i = threadIdx.x; i < 3 * kAwbBins; i += kThreads) (&s->awb_hist[0][0])[i] = 0U;
+  const Span<unsigned int> bins = sub_span(s, &s->awb_hist[0][0], 3 * kAwbBins);
+  for (int i = threadIdx.x; i < 3 * kAwbBins; i += kThreads) bins[i] = 0U;
   if (threadIdx.x < 3) s->awb_sum[threadIdx.x] = 0;
   if (threadIdx.x == 3) s->awb_quads = 0;
   if (threadIdx.x == 4) s->awb_done = 0;
@@ -581,7 +603,7 @@ __device__ void finish_stats(const FrameDesc& p, const u64 sum[3], u64 saturated
     next_gain = wanted / next_exposure;
     next_gain = next_gain < p.ae.min_gain ? p.ae.min_gain : next_gain > p.ae.max_gain ? p.ae.max_gain : next_gain;
   }
-  float* out = p.stats_out;
+  Span<float> out = p.stats_out;
   out[0] = static_cast<float>(mean[0]);
   out[1] = static_cast<float>(mean[1]);
   out[2] = static_cast<float>(mean[2]);
@@ -601,13 +623,13 @@ __device__ void finish_stats(const FrameDesc& p, const u64 sum[3], u64 saturated
 // Per-tile state the phases share.
 struct TileCtx {
   int x0, y0;
-  const uint8_t* box;
-  const int* col_mx;
-  const int* row_my;
-  const int* row_k;
-  const float* row_ty;
-  const float2* table;  // paired lens shading table
-  const float* grid;     // the frame's lens shading gains
+  Span<const uint8_t> box;
+  Span<const int> col_mx;
+  Span<const int> row_my;
+  Span<const int> row_k;
+  Span<const float> row_ty;
+  Span<const float2> table;  // paired lens shading table
+  Span<const float> grid;     // the frame's lens shading gains
   LscTile lt;
 };
 

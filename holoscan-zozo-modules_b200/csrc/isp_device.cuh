@@ -32,28 +32,28 @@ __device__ __forceinline__ float clamp01(float v) { return v < 0.0F ? 0.0F : v >
 
 // One sample's raw counts (isp_math.hpp:101-119), read through the read-only path.
 __device__ __forceinline__ int load_raw(const FrameDesc& p, int x, int y) {
-  const uint8_t* row = p.raw + static_cast<int64_t>(y) * p.raw_pitch;
+  Span<const uint8_t> row = p.raw + static_cast<int64_t>(y) * p.raw_pitch;
   switch (p.raw_format) {
     case kRawU8:
-      return __ldg(row + x);
+      return __ldg(&row[x]);
     case kRawU16:
-      return __ldg(reinterpret_cast<const uint16_t*>(row) + x);
+      return __ldg(&span_cast<const uint16_t>(row)[x]);
     case kRawRaw10: {
-      const uint8_t* g = row + 5 * (x >> 2);
+      Span<const uint8_t> g = row + 5 * (x >> 2);
       const int k = x & 3;
-      return (static_cast<int>(__ldg(g + k)) << 2) | ((__ldg(g + 4) >> (2 * k)) & 3);
+      return (static_cast<int>(__ldg(&g[k])) << 2) | ((__ldg(&g[4]) >> (2 * k)) & 3);
     }
     default: {
-      const uint8_t* g = row + 3 * (x >> 1);
+      Span<const uint8_t> g = row + 3 * (x >> 1);
       const int k = x & 1;
-      return (static_cast<int>(__ldg(g + k)) << 4) | ((__ldg(g + 2) >> (4 * k)) & 15);
+      return (static_cast<int>(__ldg(&g[k])) << 4) | ((__ldg(&g[2]) >> (4 * k)) & 15);
     }
   }
 }
 
 // Lens shading gain at (x, y) (isp_math.hpp:121-140): bilinear in the grid,
 // first across (top and bottom rows of the cell), then down.
-__device__ __forceinline__ float lens_shading_gain(const FrameDesc& p, const float* grid, int x, int y,
+__device__ __forceinline__ float lens_shading_gain(const FrameDesc& p, Span<const float> grid, int x, int y,
                                                    int channel) {
   const float fx = static_cast<float>(x) * p.lsc_sx;
   const float fy = static_cast<float>(y) * p.lsc_sy;
@@ -65,14 +65,14 @@ __device__ __forceinline__ float lens_shading_gain(const FrameDesc& p, const flo
   const float ty = fy - static_cast<float>(iy);
   const int step = p.lsc_channels;
   const int row = p.lsc_width * step;
-  const float* g = grid + (iy * p.lsc_width + ix) * step + (step == 4 ? channel : 0);
+  Span<const float> g = grid + (iy * p.lsc_width + ix) * step + (step == 4 ? channel : 0);
   const float top = g[0] + (g[step] - g[0]) * tx;
   const float bottom = g[row] + (g[row + step] - g[row]) * tx;
   return top + (bottom - top) * ty;
 }
 
 // Black level and lens shading (isp_math.hpp:144-148): 0 at black, 1 at white.
-__device__ __forceinline__ float linearize(const FrameDesc& p, const float* grid, int raw, int x, int y,
+__device__ __forceinline__ float linearize(const FrameDesc& p, Span<const float> grid, int raw, int x, int y,
                                            int channel) {
   float v = (static_cast<float>(raw) - p.black[channel]) * p.inv_range[channel];
   v = v > 0.0F ? v : 0.0F;
@@ -241,7 +241,7 @@ __device__ __forceinline__ void correct_color(const float* ccm, const float in[3
 // Tone curve (isp_math.hpp:235-243) from the table of (lut[i], lut[i+1] -
 // lut[i]) pairs, whose differences the host formed with the same float
 // subtraction: lut[i] + t * (lut[i+1] - lut[i]).
-__device__ __forceinline__ float tone(const float2* table, int size, float last, float x) {
+__device__ __forceinline__ float tone(Span<const float2> table, int size, float last, float x) {
   const float f = x * static_cast<float>(size - 1);
   const int i = static_cast<int>(f);
   if (i >= size - 1) return last;

@@ -20,7 +20,13 @@ __global__ void isp_wait_check_kernel(Scratch* scratch, unsigned int polls) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&bar)), "r"(16U) : "memory");
   }
   __syncthreads();
-  if (!mbar_wait(&bar, 0, polls) && threadIdx.x == 0) report_wait_timeout(scratch);
+  if (!mbar_wait(&bar, 0, polls) && threadIdx.x == 0) {
+#ifdef ISP_CHECKED
+    report_wait_timeout(make_span(scratch, 1, &scratch->check));
+#else
+    report_wait_timeout(scratch);
+#endif
+  }
 }
 
 }  // namespace

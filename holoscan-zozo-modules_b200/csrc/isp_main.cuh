@@ -14,40 +14,42 @@ namespace {
 
 // Shared memory of a CTA, carved from one dynamic allocation.
 struct TileSmem {
-  uint8_t* box;
-  float2* P;  // paired samples
-  float2* R;  // paired RGB planes (sharpening)
-  float2* G;
-  float2* B;
-  float2* table;  // paired lens shading table
-  int* col_mx;
-  int* col_ix;
-  float* col_tx;
-  int* row_my;
-  int* row_k;
-  float* row_ty;
-  unsigned int* hist;
-  float* grid;
-  float2* lut_s;
+  Span<uint8_t> box;
+  Span<float2> P;  // paired samples
+  Span<float2> R;  // paired RGB planes (sharpening)
+  Span<float2> G;
+  Span<float2> B;
+  Span<float2> table;  // paired lens shading table
+  Span<int> col_mx;
+  Span<int> col_ix;
+  Span<float> col_tx;
+  Span<int> row_my;
+  Span<int> row_k;
+  Span<float> row_ty;
+  Span<unsigned int> hist;
+  Span<float> grid;
+  Span<float2> lut_s;
 };
 
-__device__ __forceinline__ TileSmem carve(unsigned char* smem, const Layout& L, int sample_rows) {
+// Each region spans the bytes up to the next (the checked build holds its
+// accesses to them; `rec` is where it counts violations).
+__device__ __forceinline__ TileSmem carve(unsigned char* smem, const Layout& L, int sample_rows, CheckRecord* rec) {
   TileSmem m;
-  m.box = smem + L.raw;
-  m.P = reinterpret_cast<float2*>(smem + L.samples);
-  m.R = reinterpret_cast<float2*>(smem + L.r);
-  m.G = reinterpret_cast<float2*>(smem + L.g);
-  m.B = reinterpret_cast<float2*>(smem + L.b);
-  m.table = reinterpret_cast<float2*>(smem + L.lsc);
-  m.col_mx = reinterpret_cast<int*>(smem + L.cols);
-  m.col_ix = m.col_mx + kSW;
-  m.col_tx = reinterpret_cast<float*>(m.col_ix + kSW);
-  m.row_my = reinterpret_cast<int*>(smem + L.rows);
-  m.row_k = m.row_my + sample_rows;
-  m.row_ty = reinterpret_cast<float*>(m.row_k + sample_rows);
-  m.hist = reinterpret_cast<unsigned int*>(smem + L.hist);
-  m.grid = reinterpret_cast<float*>(smem + L.grid);
-  m.lut_s = reinterpret_cast<float2*>(smem + L.lut);
+  m.box = carve_span<uint8_t>(smem, L.raw, L.samples - L.raw, rec);
+  m.P = carve_span<float2>(smem, L.samples, L.r - L.samples, rec);
+  m.R = carve_span<float2>(smem, L.r, L.g - L.r, rec);
+  m.G = carve_span<float2>(smem, L.g, L.b - L.g, rec);
+  m.B = carve_span<float2>(smem, L.b, L.lsc - L.b, rec);
+  m.table = carve_span<float2>(smem, L.lsc, L.cols - L.lsc, rec);
+  m.col_mx = carve_span<int>(smem, L.cols, kSW * 4, rec);
+  m.col_ix = carve_span<int>(smem, L.cols + kSW * 4, kSW * 4, rec);
+  m.col_tx = carve_span<float>(smem, L.cols + 2 * kSW * 4, kSW * 4, rec);
+  m.row_my = carve_span<int>(smem, L.rows, sample_rows * 4, rec);
+  m.row_k = carve_span<int>(smem, L.rows + sample_rows * 4, sample_rows * 4, rec);
+  m.row_ty = carve_span<float>(smem, L.rows + 2 * sample_rows * 4, sample_rows * 4, rec);
+  m.hist = carve_span<unsigned int>(smem, L.hist, L.grid - L.hist, rec);
+  m.grid = carve_span<float>(smem, L.grid, L.lut - L.grid, rec);
+  m.lut_s = carve_span<float2>(smem, L.lut, L.total - L.lut, rec);
   return m;
 }
 
@@ -57,8 +59,8 @@ struct FrameSetup {
   float qblack[4];  // per quad position
   float qinv[4];
   float qgain[4];
-  const float2* lut;
-  const float* grid;  // lens shading gains: shared memory when they fit
+  Span<const float2> lut;
+  Span<const float> grid;  // lens shading gains: shared memory when they fit
   float lut_scale;
   bool swap_rb;
   bool want_hist;
@@ -149,7 +151,7 @@ __device__ __forceinline__ void unit_rc(int u, bool same_parity, int& r, int& uc
 // fixed at compile time (the single-frame kernels), or -1 to choose it per
 // unit (the batch kernel).
 template <int kOutSel, bool kLutSmem>
-__device__ __forceinline__ void finish_row(const FrameDesc& p, const FrameSetup& f, unsigned int* hist,
+__device__ __forceinline__ void finish_row(const FrameDesc& p, const FrameSetup& f, Span<unsigned int> hist,
                                            const float2 (&rgb)[4][3], int x, int y, unsigned int (&sums)[3],
                                            unsigned int& npix) {
   if (y >= p.height) return;
@@ -204,10 +206,10 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
   t.table = m.table;
   t.grid = f.grid;
   t.lt = interior ? build_lsc_inner(p, f.grid, p.pattern, x0 - 4, y0 - G::kHalo, G::kSH, m.col_mx, m.col_ix,
-                                    m.col_tx, m.row_my, m.row_k, m.row_ty, reinterpret_cast<float*>(m.table), minmax)
+                                    m.col_tx, m.row_my, m.row_k, m.row_ty, span_cast<float>(m.table), minmax)
                   : build_lsc<true>(p, f.grid, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, true, p.width + 3,
                                     p.height + G::kHalo - 1, m.col_mx, m.col_ix, m.col_tx, m.row_my, m.row_k, m.row_ty,
-                                    reinterpret_cast<float*>(m.table), minmax);
+                                    span_cast<float>(m.table), minmax);
   if (use_tma) {
     if (!mbar_wait(bar, phase) && tid == 0) report_wait_timeout(p.scratch);
     phase ^= 1U;
@@ -316,9 +318,9 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
 // into the frame's scratch; the CTA that completes the frame's tile count
 // writes the user's histogram and statistics and clears the scratch (and
 // the tile claims of the single-frame pass). `red` holds 4 x kWarps values.
-__device__ void flush_frame(const FrameDesc& p, const FrameSetup& f, const u64 (&acc)[4], unsigned int* hist,
+__device__ void flush_frame(const FrameDesc& p, const FrameSetup& f, const u64 (&acc)[4], Span<unsigned int> hist,
                             u64* red, bool* last, unsigned int tiles_done, unsigned int tiles_total) {
-  Scratch* sc = p.scratch;
+  Span<Scratch> sc = p.scratch;
   const int tid = threadIdx.x;
   if (!f.want_stats && !f.want_hist) {
     // Nothing to finish, but the last CTA still clears the counters.
@@ -339,12 +341,11 @@ __device__ void flush_frame(const FrameDesc& p, const FrameSetup& f, const u64 (
     // Two bins per 64-bit atomic: a bin's count over a frame stays below
     // 2^32, so no carry crosses into its neighbour.
     static_assert(offsetof(Scratch, hist) % 8 == 0, "histogram pairs are 8-byte aligned");
+    const Span<unsigned long long> pairs =
+        span_cast<unsigned long long>(sub_span(sc, &sc->hist[0], kHistChannels * kHistBins));
     for (int i = tid; i < kHistChannels * kHistBins / 2; i += kThreads) {
-      const uint2 h = reinterpret_cast<const uint2*>(hist)[i];
-      if ((h.x | h.y) != 0U) {
-        atomicAdd(reinterpret_cast<unsigned long long*>(&sc->hist[2 * i]),
-                  (static_cast<unsigned long long>(h.y) << 32) | h.x);
-      }
+      const uint2 h = span_cast<const uint2>(hist)[i];
+      if ((h.x | h.y) != 0U) atomicAdd(&pairs[i], (static_cast<unsigned long long>(h.y) << 32) | h.x);
     }
   }
   __threadfence();
@@ -354,9 +355,10 @@ __device__ void flush_frame(const FrameDesc& p, const FrameSetup& f, const u64 (
   if (!*last) return;
   __threadfence();
   if (f.want_hist) {
+    const Span<unsigned int> bins = sub_span(sc, &sc->hist[0], kHistChannels * kHistBins);
     for (int i = tid; i < kHistChannels * kHistBins; i += kThreads) {
-      p.hist_out[i] = __ldcg(&sc->hist[i]);
-      sc->hist[i] = 0U;
+      p.hist_out[i] = __ldcg(&bins[i]);
+      bins[i] = 0U;
     }
   }
   if (f.want_stats && tid == 0) {
@@ -379,7 +381,8 @@ __global__ void __launch_bounds__(kThreads, kTileH == kTH ? 2 : 3)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128U - (smem_u32(smem_raw) & 127U)) & 127U);
   const int box_bytes = box_row_bytes(p.raw_format);
-  const TileSmem m = carve(smem, layout_of(kSharpen, box_bytes, kLutSmem ? p.tone_size : 0, kTileH), G::kSH);
+  const TileSmem m =
+      carve(smem, layout_of(kSharpen, box_bytes, kLutSmem ? p.tone_size : 0, kTileH), G::kSH, span_rec(p.scratch));
   __shared__ uint64_t bar;
   __shared__ u64 red[4 * kWarps];
   __shared__ int minmax[2];

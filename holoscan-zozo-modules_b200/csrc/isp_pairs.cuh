@@ -42,9 +42,9 @@ __device__ __forceinline__ int psw(int j) { return ((j >> 1) & 1) << 1; }
 __device__ __forceinline__ int csw(int j) { return (j >> 1) & 1; }
 __device__ __forceinline__ int cchunk(int c, int sw) { return c < kCW2 / 2 - 1 ? c ^ sw : c; }
 
-__device__ __forceinline__ float4 lds4(const float2* p) { return *reinterpret_cast<const float4*>(p); }
-__device__ __forceinline__ void sts4(float2* p, float2 a, float2 b) {
-  *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+__device__ __forceinline__ float4 lds4(Span<const float2> p) { return *span_cast<const float4>(p); }
+__device__ __forceinline__ void sts4(Span<float2> p, float2 a, float2 b) {
+  *span_cast<float4>(p) = make_float4(a.x, a.y, b.x, b.y);
 }
 __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
@@ -54,7 +54,7 @@ __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); 
 //    once. kSrc: 0 interior tile from the TMA box, 1 edge tile from the box
 //    (mirrored columns), 2 no box (global loads, mirrored).
 template <int kFmt, int kSrc, int kHalo, int kTileH>
-__device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileCtx& t, float2* P, int box_bytes,
+__device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileCtx& t, Span<float2> P, int box_bytes,
                                                  const float (&qblack)[4], const float (&qinv)[4],
                                                  const float (&qgain)[4], bool want_stats) {
   constexpr int kSH = kTileH + 2 * kHalo;
@@ -66,11 +66,11 @@ __device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileC
     const int par = j & 1;  // row parity: y0 - halo is even
     unsigned int sl[4], sr[4];  // samples 4u + k and 4u + 32 + k
     if constexpr (kSrc == 0) {
-      const uint8_t* row = t.box + j * box_bytes;
+      Span<const uint8_t> row = t.box + j * box_bytes;
       unpack4(kFmt, row, u, sl);
       unpack4(kFmt, row, u + kHalf / 4, sr);
     } else if constexpr (kSrc == 1) {
-      const uint8_t* row = t.box + (t.row_my[j] - (t.y0 - kHalo)) * box_bytes;
+      Span<const uint8_t> row = t.box + (t.row_my[j] - (t.y0 - kHalo)) * box_bytes;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         sl[k] = unpack1(kFmt, row, t.col_mx[4 * u + k], t.x0);
@@ -115,8 +115,8 @@ __device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileC
       if (t.lt.rows <= kLscTableRows) {
         const int kk = t.row_k[j];
         const int pl = p.lsc_channels == 4 ? par : 0;
-        const float2* r0 = t.table + (kk * 2 + pl) * kPW + 4 * u;
-        const float2* r1 = t.table + ((kk + 1) * 2 + pl) * kPW + 4 * u;
+        Span<const float2> r0 = t.table + (kk * 2 + pl) * kPW + 4 * u;
+        Span<const float2> r1 = t.table + ((kk + 1) * 2 + pl) * kPW + 4 * u;
         const float4 a0 = lds4(r0), b0 = lds4(r0 + 2), a1 = lds4(r1), b1 = lds4(r1 + 2);
         const float2 t0[4] = {lo2(a0), hi2(a0), lo2(b0), hi2(b0)};
         const float2 t1[4] = {lo2(a1), hi2(a1), lo2(b1), hi2(b1)};
@@ -135,7 +135,7 @@ __device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileC
       }
     }
     // White balance and the clip to 1 (v >= 0): the saturating multiply.
-    float2* dst = P + j * kPW;
+    Span<float2> dst = P + j * kPW;
     const int sw = psw(j);
     sts4(dst + ((4 * u) ^ sw), mul_sat2(v[0], bc2(gn0)), mul_sat2(v[1], bc2(gn1)));
     sts4(dst + ((4 * u + 2) ^ sw), mul_sat2(v[2], bc2(gn0)), mul_sat2(v[3], bc2(gn1)));
@@ -144,7 +144,7 @@ __device__ __forceinline__ unsigned int phase_a2(const FrameDesc& p, const TileC
 }
 
 template <int kSrc, int kHalo, int kTileH>
-__device__ __forceinline__ unsigned int phase_a2_fmt(const FrameDesc& p, const TileCtx& t, float2* P, int box_bytes,
+__device__ __forceinline__ unsigned int phase_a2_fmt(const FrameDesc& p, const TileCtx& t, Span<float2> P, int box_bytes,
                                                      const float (&qblack)[4], const float (&qinv)[4],
                                                      const float (&qgain)[4], bool want_stats) {
   // Global loads (no TMA box) read the format at run time in load_raw.
@@ -165,7 +165,7 @@ __device__ __forceinline__ unsigned int phase_a2_fmt(const FrameDesc& p, const T
 //    demosaic runs as the layout's canonical pattern (RGGB or GRBG), and
 //    BGGR and GBRG trade red and blue.
 template <bool kMalvar, int kPat, int kTileH>
-__device__ __forceinline__ void phase_b2(const float2* P, float2* R, float2* G, float2* B) {
+__device__ __forceinline__ void phase_b2(Span<const float2> P, Span<float2> R, Span<float2> G, Span<float2> B) {
   constexpr int kUnitsQ = kCW2 / 2;                   // 17
   constexpr int kUnits = (kTileH + 2) / 2 * kUnitsQ;  // 33 x 17 for 64 rows
   for (int unit = threadIdx.x; unit < kUnits; unit += kThreads) {
@@ -178,7 +178,7 @@ __device__ __forceinline__ void phase_b2(const float2* P, float2* R, float2* G, 
 #pragma unroll
     for (int a = 0; a < 6; ++a) {
       const int j = 2 * ur + 1 + a;
-      const float2* row = P + j * kPW;  // pair 2uq is w column -1
+      Span<const float2> row = P + j * kPW;  // pair 2uq is w column -1
       const int sw = psw(j);
       const bool edge = a == 0 || a == 5;
       const bool mid = a == 2 || a == 3;
@@ -222,14 +222,14 @@ __device__ __forceinline__ void phase_b2(const float2* P, float2* R, float2* G, 
 // of output rows r and r + 1, sharpened: RGB rows r .. r + 3 (each loaded
 // once for both output rows), pair columns 4uc .. 4uc + 5 (chunks 2uc ..
 // 2uc + 2, stored at chunk ^ csw(row)).
-__device__ __forceinline__ void sharpen_rows2(const float2* X, int r, int uc, float2 amount, float2 (&o0)[4],
+__device__ __forceinline__ void sharpen_rows2(Span<const float2> X, int r, int uc, float2 amount, float2 (&o0)[4],
                                               float2 (&o1)[4]) {
   float2 w[4][6];
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     const int j = r + a;
     const int s = csw(j);
-    const float2* row = X + j * kCW2;
+    Span<const float2> row = X + j * kCW2;
     const float4 v0 = lds4(row + 2 * ((2 * uc) ^ s)), v1 = lds4(row + 2 * ((2 * uc + 1) ^ s)),
                  v2 = lds4(row + 2 * cchunk(2 * uc + 2, s));
     w[a][0] = lo2(v0);
@@ -252,13 +252,13 @@ __device__ __forceinline__ void sharpen_rows2(const float2* X, int r, int uc, fl
 // 4uc .. 4uc + 3 of output row r, sharpened from RGB rows r .. r + 2 (loaded
 // as in sharpen_rows2; a quarter-warp takes rows r and r + 2, which csw
 // sends to different banks).
-__device__ __forceinline__ void sharpen_row1(const float2* X, int r, int uc, float2 amount, float2 (&o)[4]) {
+__device__ __forceinline__ void sharpen_row1(Span<const float2> X, int r, int uc, float2 amount, float2 (&o)[4]) {
   float2 w[3][6];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const int j = r + a;
     const int s = csw(j);
-    const float2* row = X + j * kCW2;
+    Span<const float2> row = X + j * kCW2;
     const float4 v0 = lds4(row + 2 * ((2 * uc) ^ s)), v1 = lds4(row + 2 * ((2 * uc + 1) ^ s)),
                  v2 = lds4(row + 2 * cchunk(2 * uc + 2, s));
     w[a][0] = lo2(v0);
@@ -279,11 +279,11 @@ __device__ __forceinline__ void sharpen_row1(const float2* X, int r, int uc, flo
 // from the samples: sample rows r .. r + 4 (halo 2), pair columns 4uc + 2 ..
 // 4uc + 9. kRowPar: the parity of the output row.
 template <bool kMalvar, int kPat, int kRowPar>
-__device__ __forceinline__ void demosaic_row4(const float2* P, int r, int uc, float2 (&rgb)[4][3]) {
+__device__ __forceinline__ void demosaic_row4(Span<const float2> P, int r, int uc, float2 (&rgb)[4][3]) {
   float2 w[5][8] = {};
 #pragma unroll
   for (int a = 0; a < 5; ++a) {
-    const float2* row = P + (r + a) * kPW;
+    Span<const float2> row = P + (r + a) * kPW;
     const int sw = psw(r + a);
     const int s0 = 4 * uc + 2;
     const bool edge = a == 0 || a == 4;
@@ -327,8 +327,12 @@ __device__ __forceinline__ void demosaic_row4(const float2* P, int r, int uc, fl
 // last entry's difference is -0.0, so x = 1 (t = +0) returns lut[N-1]
 // exactly, as the reference's branch does, whatever the sign of lut[N-1].
 template <bool kLutSmem>
-__device__ __forceinline__ float tone_lookup(const float2* table, float m, float frac) {
+__device__ __forceinline__ float tone_lookup(Span<const float2> table, float m, float frac) {
   float2 e;
+#ifdef ISP_CHECKED
+  // Entry trunc(f) through the checked span.
+  e = table[static_cast<int>(__float_as_uint(m) - kTwo23Bits)];
+#else
   if constexpr (kLutSmem) {
     // Shared address of entry trunc(f): base + 8 (bits - 2^23 bits), wrapping.
     const uint32_t addr = smem_u32(table) + (__float_as_uint(m) << 3) - (kTwo23Bits << 3);
@@ -336,6 +340,7 @@ __device__ __forceinline__ float tone_lookup(const float2* table, float m, float
   } else {
     e = __ldg(table + magic_int(m));
   }
+#endif
   return fadd(e.x, fmul(frac, e.y));
 }
 
@@ -345,8 +350,8 @@ __device__ __forceinline__ float tone_lookup(const float2* table, float m, float
 // 8-bit histogram codes (isp_math.hpp:279-305). `n`: pixels inside the image.
 template <int kOut>
 __device__ __forceinline__ void store_seg4(const FrameDesc& p, int x, int y, const float (&t)[4][3],
-                                           const unsigned int (&c)[4][3], int n, bool want_hist, unsigned int* hist) {
-  uint8_t* row = p.out + static_cast<int64_t>(y) * p.out_pitch;
+                                           const unsigned int (&c)[4][3], int n, bool want_hist, Span<unsigned int> hist) {
+  Span<uint8_t> row = p.out + static_cast<int64_t>(y) * p.out_pitch;
   const bool vec = n == 4 && p.out_vector;
   unsigned int q[4][3];  // histogram codes
   if constexpr (kOut == kOutRgb8 || kOut == kOutRgba8) {
@@ -357,7 +362,7 @@ __device__ __forceinline__ void store_seg4(const FrameDesc& p, int x, int y, con
     }
     if constexpr (kOut == kOutRgb8) {
       if (vec) {
-        unsigned int* o = reinterpret_cast<unsigned int*>(row + 3 * x);
+        Span<unsigned int> o = span_cast<unsigned int>(row + 3 * x);
         o[0] = __byte_perm(__byte_perm(c[0][0], c[0][1], 0x0040), __byte_perm(c[0][2], c[1][0], 0x0040), 0x5410);
         o[1] = __byte_perm(__byte_perm(c[1][1], c[1][2], 0x0040), __byte_perm(c[2][0], c[2][1], 0x0040), 0x5410);
         o[2] = __byte_perm(__byte_perm(c[2][2], c[3][0], 0x0040), __byte_perm(c[3][1], c[3][2], 0x0040), 0x5410);
@@ -376,7 +381,7 @@ __device__ __forceinline__ void store_seg4(const FrameDesc& p, int x, int y, con
         w[d] = __byte_perm(__byte_perm(c[d][0], c[d][1], 0x0040), c[d][2], 0x7410) | 0xFF000000U;
       }
       if (vec) {
-        *reinterpret_cast<uint4*>(row + 4 * x) = make_uint4(w[0], w[1], w[2], w[3]);
+        *span_cast<uint4>(row + 4 * x) = make_uint4(w[0], w[1], w[2], w[3]);
       } else {
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
@@ -398,12 +403,12 @@ __device__ __forceinline__ void store_seg4(const FrameDesc& p, int x, int y, con
       }
     }
     if (vec) {
-      uint2* o = reinterpret_cast<uint2*>(row + 6 * x);
+      Span<uint2> o = span_cast<uint2>(row + 6 * x);
       o[0] = make_uint2(__byte_perm(c[0][0], c[0][1], 0x5410), __byte_perm(c[0][2], c[1][0], 0x5410));
       o[1] = make_uint2(__byte_perm(c[1][1], c[1][2], 0x5410), __byte_perm(c[2][0], c[2][1], 0x5410));
       o[2] = make_uint2(__byte_perm(c[2][2], c[3][0], 0x5410), __byte_perm(c[3][1], c[3][2], 0x5410));
     } else {
-      uint16_t* o = reinterpret_cast<uint16_t*>(row);
+      Span<uint16_t> o = span_cast<uint16_t>(row);
 #pragma unroll
       for (int d = 0; d < 4; ++d) {
         if (d >= n) break;
@@ -418,12 +423,12 @@ __device__ __forceinline__ void store_seg4(const FrameDesc& p, int x, int y, con
       for (int k = 0; k < 3; ++k) q[d][k] = c[d][k] & 0xFFU;
     }
     if (vec) {
-      float4* o = reinterpret_cast<float4*>(row + 12 * x);
+      Span<float4> o = span_cast<float4>(row + 12 * x);
       o[0] = make_float4(t[0][0], t[0][1], t[0][2], t[1][0]);
       o[1] = make_float4(t[1][1], t[1][2], t[2][0], t[2][1]);
       o[2] = make_float4(t[2][2], t[3][0], t[3][1], t[3][2]);
     } else {
-      float* o = reinterpret_cast<float*>(row);
+      Span<float> o = span_cast<float>(row);
 #pragma unroll
       for (int d = 0; d < 4; ++d) {
         if (d >= n) break;
@@ -454,8 +459,8 @@ __device__ __forceinline__ void store_seg4(const FrameDesc& p, int x, int y, con
 // caller subtracts npix x 2^23 bits.
 template <int kOut, bool kLutSmem, bool kFull>
 __device__ __forceinline__ void finish_pairs(const FrameDesc& p, const float2 (&rgb)[4][3], int x, int y, int nl_,
-                                             int nr_, const float2* lut, float lut_scale, bool want_stats,
-                                             bool want_hist, unsigned int* hist, unsigned int (&sums)[3],
+                                             int nr_, Span<const float2> lut, float lut_scale, bool want_stats,
+                                             bool want_hist, Span<unsigned int> hist, unsigned int (&sums)[3],
                                              unsigned int& npix) {
   const int nl = kFull ? 4 : nl_;
   const int nr = kFull ? 4 : nr_;
@@ -505,8 +510,8 @@ __device__ __forceinline__ void finish_pairs(const FrameDesc& p, const float2 (&
 
 template <bool kLutSmem, bool kFull>
 __device__ __forceinline__ void finish_pairs_any(const FrameDesc& p, const float2 (&rgb)[4][3], int x, int y, int nl,
-                                                 int nr, const float2* lut, float lut_scale, bool want_stats,
-                                                 bool want_hist, unsigned int* hist, unsigned int (&sums)[3],
+                                                 int nr, Span<const float2> lut, float lut_scale, bool want_stats,
+                                                 bool want_hist, Span<unsigned int> hist, unsigned int (&sums)[3],
                                                  unsigned int& npix) {
   switch (p.out_format) {
     case kOutRgb8:

@@ -5,6 +5,8 @@
 
 #include <cstdint>
 
+#include "isp_checked.cuh"
+
 namespace isp_b200 {
 
 // Channels of the mosaic (isp_params.hpp:65-68) and sample/output formats.
@@ -42,6 +44,9 @@ struct Scratch {
   int error;  // a bounded wait in a kernel gave up (1)
   unsigned int tile_next;  // the single-frame tile pass's tiles claimed beyond the first one per CTA
   unsigned int pad;
+#ifdef ISP_CHECKED
+  CheckRecord check;  // out-of-bounds accesses refused by the checked build
+#endif
 };
 
 struct AutoExposure {
@@ -58,7 +63,7 @@ struct AutoExposure {
 struct FrameDesc {
   int width;
   int height;
-  const uint8_t* raw;
+  Span<const uint8_t> raw;
   int64_t raw_pitch;
   int raw_format;
   int pattern;
@@ -68,24 +73,24 @@ struct FrameDesc {
   int white;
   float wb[3];
   int auto_wb;  // gains from scratch->awb_gains
-  const float* lsc;  // lens shading grid in device memory, or null
+  Span<const float> lsc;  // lens shading grid in device memory, or null
   int lsc_width;
   int lsc_height;
   int lsc_channels;
   float lsc_sx;
   float lsc_sy;
   float ccm[9];
-  const float2* tone;  // (lut[i], lut[i+1] - lut[i]) pairs in device memory
+  Span<const float2> tone;  // (lut[i], lut[i+1] - lut[i]) pairs in device memory
   int tone_size;
   float tone_last;
   float sharpen;
-  uint8_t* out;
+  Span<uint8_t> out;
   int64_t out_pitch;
   int out_format;
   int out_vector;  // out and out_pitch allow the kernels' vector stores
-  uint32_t* hist_out;  // user histogram [4][256], or null
-  float* stats_out;    // user statistics [12], or null
-  Scratch* scratch;
+  Span<uint32_t> hist_out;  // user histogram [4][256], or null
+  Span<float> stats_out;    // user statistics [12], or null
+  Span<Scratch> scratch;
   AutoExposure ae;
   int64_t exposure_ns;
   float exposure_gain;

@@ -22,7 +22,14 @@ from . import abi
 from .abi import IspParams, RawFrame  # noqa: F401  (re-exported)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "libisp_b200.so")
+# ISP_B200_LIBRARY=checked selects the bounds-checked build of the ISP
+# (libisp_b200_checked.so: every shared- and global-memory access of its
+# kernels checked, refused accesses counted per pipeline).
+CHECKED = os.environ.get("ISP_B200_LIBRARY", "") == "checked"
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libisp_b200_checked.so" if CHECKED else "libisp_b200.so")
+# Pipelines the checked build refused accesses for, as (what, count, first
+# address), recorded when they close.
+VIOLATIONS = []
 
 _lib = None
 
@@ -72,6 +79,7 @@ def lib() -> C.CDLL:
         L.isp_b200_device_status.argtypes = [C.c_void_p, P(C.c_int32)]
         L.isp_b200_set_kernel_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.isp_b200_check_bounded_wait.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        L.isp_b200_checked_violations.argtypes = [C.c_void_p, P(C.c_uint32), P(C.c_uint64)]
         L.isp_b200_set_frame_overlap.argtypes = [C.c_void_p, C.c_int32]
         L.isp_b200_process_host.argtypes = [C.c_void_p, P(abi.RawViewC), P(abi.RgbViewC), P(abi.StatsC),
                                             P(abi.ExposureC)]
@@ -172,6 +180,10 @@ class Pipeline:
 
     def close(self) -> None:
         if getattr(self, "handle", None):
+            if CHECKED:
+                count, first = self.checked_violations()
+                if count:
+                    VIOLATIONS.append((repr(self.params)[:200], count, hex(first)))
             lib().isp_b200_destroy(self.handle)
             self.handle = None
 
@@ -186,6 +198,14 @@ class Pipeline:
 
     def __exit__(self, *exc):
         self.close()
+
+    def checked_violations(self) -> Tuple[int, int]:
+        """(count, first address) of the accesses the checked build refused on this camera's frames since
+        the last call; raises ValueError (ISP_EINVAL) with the regular library, which checks nothing."""
+        count = C.c_uint32()
+        first = C.c_uint64()
+        check(lib().isp_b200_checked_violations(self.handle, C.byref(count), C.byref(first)))
+        return int(count.value), int(first.value)
 
     def reset(self) -> None:
         check(lib().isp_b200_reset(self.handle))

@@ -467,6 +467,17 @@ ISP_B200_API int isp_b200_device_status(isp_b200_pipeline* pipeline, int32_t* st
  * and the pipeline's next frame is unaffected. */
 ISP_B200_API int isp_b200_check_bounded_wait(isp_b200_pipeline* pipeline, uint32_t polls, void* stream);
 
+/* Out-of-bounds report of the bounds-checked build, no reference counterpart
+ * (the reference runs its tests under compute-sanitizer instead,
+ * modules/isp/tests/CMakeLists.txt:34-50). libisp_b200_checked.so is this
+ * library compiled with every shared- and global-memory access of the ISP
+ * kernels checked against the extent of the array it indexes; an access
+ * outside it is not made and is counted instead. This call waits for the
+ * pipeline's queued frames, then reports (and clears) how many accesses were
+ * refused since the last call and the address of the first (0 when none).
+ * The regular library returns ISP_EINVAL: it makes no checks. */
+ISP_B200_API int isp_b200_checked_violations(isp_b200_pipeline* pipeline, uint32_t* count, uint64_t* first_address);
+
 /* Profiling hook, no reference counterpart: events (cudaEvent_t, may be null)
  * that every following process call records on its stream right before and
  * right after the fused tile kernel, so a caller can time that kernel alone. */

@@ -15,3 +15,21 @@ for path in (ROOT, os.path.join(ROOT, "holoscan-zozo-modules_b200"), os.path.joi
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (a B200) and the built sm_100a library")
+
+
+if os.environ.get("ISP_B200_LIBRARY", "") == "checked":
+    import gc
+
+    import pytest
+
+    @pytest.fixture(autouse=True)
+    def _no_checked_violations():
+        """Under the bounds-checked library every pipeline a test closed (or
+        dropped) must have had no access refused."""
+        import isp_b200
+
+        yield
+        gc.collect()
+        found = list(isp_b200.VIOLATIONS)
+        isp_b200.VIOLATIONS.clear()
+        assert not found, f"out-of-bounds accesses refused: {found}"

@@ -35,6 +35,16 @@ def test_library_exports_every_declared_symbol(header, prefix, least):
     assert lib.isp_b200_abi_version() == abi.ABI_VERSION
 
 
+def test_checked_library_exports_every_isp_symbol():
+    """libisp_b200_checked.so (the bounds-checked build) is a drop-in for the ISP part of the library."""
+    lib = C.CDLL(os.path.join(ROOT, "holoscan-zozo-modules_b200", "libisp_b200_checked.so"))
+    for name in declared_functions():
+        assert hasattr(lib, name), f"{name} is declared in include/isp_b200.h but not exported by the checked build"
+    assert lib.isp_b200_abi_version() == abi.ABI_VERSION
+    count, first = C.c_uint32(7), C.c_uint64(7)
+    assert lib.isp_b200_checked_violations(None, C.byref(count), C.byref(first)) == abi.EINVAL
+
+
 def test_defaults_are_the_reference_defaults():
     c = isp_b200.params_default()
     p = abi.IspParams().to_c().c
