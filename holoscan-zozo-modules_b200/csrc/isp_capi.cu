@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -176,7 +177,16 @@ FrameDesc make_desc(const isp_params_c& p, const DeviceState& s, const isp_raw_v
   d.tone_size = s.tone_size;
   d.tone_last = s.tone_last;
   d.sharpen = p.sharpen;
-  d.out = make_span(static_cast<uint8_t*>(out.data), out.pitch * rows_before_last + out_row, rec);
+  size_t out_bytes = out.pitch * rows_before_last + out_row;
+#ifdef ISP_CHECKED
+  // Test hook of the checked build: ISP_CHECKED_SHRINK_OUTPUT=n declares the
+  // output n bytes shorter than it is, so that a frame's last stores are
+  // refused and counted (they fall inside the real buffer either way).
+  if (const char* shrink = std::getenv("ISP_CHECKED_SHRINK_OUTPUT")) {
+    out_bytes -= std::min(out_bytes, static_cast<size_t>(std::strtoull(shrink, nullptr, 10)));
+  }
+#endif
+  d.out = make_span(static_cast<uint8_t*>(out.data), out_bytes, rec);
   d.out_pitch = static_cast<int64_t>(out.pitch);
   d.out_format = out.format;
   d.out_vector = (reinterpret_cast<uintptr_t>(out.data) % 16U == 0U) && (out.pitch % 16U == 0U);
