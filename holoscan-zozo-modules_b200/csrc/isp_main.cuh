@@ -86,6 +86,13 @@ __device__ __forceinline__ void fill_frame_smem(const FrameDesc& p, const TileSm
   }
 }
 
+// The frame's lens shading gains as the tiles read them: the shared-memory
+// copy when the grid fits, else the pipeline's grid in device memory.
+__device__ __forceinline__ Span<const float> frame_grid(const FrameDesc& p, const TileSmem& m) {
+  const int gains = p.lsc_width * p.lsc_height * p.lsc_channels;
+  return p.lsc != nullptr && gains <= kGridSmemGains ? Span<const float>(m.grid) : p.lsc;
+}
+
 // Reads the frame's gains (its estimate, for auto white balance) and, with
 // kFill, fills the frame's shared memory (fill_frame_smem, its copies waited
 // for; without kFill the caller filled it before and waits for the copies).
@@ -103,8 +110,7 @@ __device__ __forceinline__ FrameSetup setup_frame(const FrameDesc& p, const Tile
     f.qinv[k] = p.inv_range[ch];
     f.qgain[k] = f.gains[color_of(ch)];
   }
-  const int gains = p.lsc_width * p.lsc_height * p.lsc_channels;
-  f.grid = p.lsc != nullptr && gains <= kGridSmemGains ? m.grid : p.lsc;
+  f.grid = frame_grid(p, m);
   f.lut = kLutSmem ? m.lut_s : p.tone;
   f.lut_scale = static_cast<float>(p.tone_size - 1);
   // The demosaic runs as the layout's canonical pattern (RGGB or GRBG); for
@@ -176,20 +182,24 @@ __device__ __forceinline__ void finish_row(const FrameDesc& p, const FrameSetup&
   }
 }
 
-// One 64x64 tile at (x0, y0). `map` is the frame's TMA descriptor (its box
-// is waited for on `bar`); after phase A, when the box is free again,
-// `after_a()` runs (to prefetch the next tile). Adds the tile's statistics
-// sums and saturated count to `acc` (per thread).
-// A hook that does nothing (run_tile's before_c by default).
+// A hook that does nothing (run_tile's default hooks).
 struct NoHook {
   __device__ __forceinline__ void operator()() const {}
 };
 
+// One 64x64 tile at (x0, y0) (kTileH rows). Its box is waited for on `bar`.
+// Hooks, all run by every thread: `after_lsc()` once the tile's lens shading
+// maps and table are built, before the box wait and phase A (the frame's
+// gains may be read there); `after_a()` after phase A, when the box is free
+// again (to claim or prefetch the next tile); `before_c()` before phase C.
+// Adds the tile's statistics sums and saturated count to `acc` (per thread).
+
 template <bool kMalvar, bool kSharpen, int kLayout, bool kLutSmem, class AfterA, int kOutSel = -1, int kTileH = kTH,
-          class BeforeC = NoHook>
+          class BeforeC = NoHook, class AfterLsc = NoHook>
 __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f, const TileSmem& m, int* minmax,
                                          int x0, int y0, bool use_tma, uint64_t* bar, uint32_t& phase,
-                                         u64 (&acc)[4], AfterA after_a, BeforeC before_c = BeforeC{}) {
+                                         u64 (&acc)[4], AfterA after_a, BeforeC before_c = BeforeC{},
+                                         AfterLsc after_lsc = AfterLsc{}) {
   using G = Geom<kSharpen, kTileH>;
   constexpr int kPat = kLayout * 2;
   const int tid = threadIdx.x;
@@ -210,6 +220,7 @@ __device__ __forceinline__ void run_tile(const FrameDesc& p, const FrameSetup& f
                   : build_lsc<true>(p, f.grid, p.pattern, x0 - 4, kSW, y0 - G::kHalo, G::kSH, true, p.width + 3,
                                     p.height + G::kHalo - 1, m.col_mx, m.col_ix, m.col_tx, m.row_my, m.row_k, m.row_ty,
                                     span_cast<float>(m.table), minmax);
+  after_lsc();
   if (use_tma) {
     if (!mbar_wait(bar, phase) && tid == 0) report_wait_timeout(p.scratch);
     phase ^= 1U;
@@ -405,20 +416,30 @@ __global__ void __launch_bounds__(kThreads, kTileH == kTH ? 2 : 3)
     if (static_cast<int>(blockIdx.x) < tiles) issue(blockIdx.x);
   }
   fill_frame_smem<kLutSmem>(p, m);
-  // Launched as a programmatic dependent of the statistics pass, this kernel
-  // becomes resident on the SMs that pass leaves while it finishes; the wait
-  // returns once the pass has completed and its writes (the gains that
-  // setup_frame reads) are visible. Without a programmatic launch it returns
-  // at once.
-  griddep_wait();
-  // The next frame's statistics pass may launch now (when queued right
-  // behind this kernel): it sums its own raw frame on the SMs this pass
-  // leaves as it finishes, and waits for this pass's completion before its
-  // estimate touches the white balance state read below.
-  griddep_launch_dependents();
-  const FrameSetup f = setup_frame<kLutSmem, false>(p, m);
+  // The frame's set-up waits for the statistics pass (its gains); the first
+  // tile's lens shading maps and table read only the pipeline's own grid, so
+  // they are built before that wait (run_tile calls wait_frame after them).
+  FrameSetup f;
+  f.grid = frame_grid(p, m);
   cp_async_wait_all();
   __syncthreads();
+  bool waited = false;
+  const auto wait_frame = [&] {
+    if (waited) return;
+    // Launched as a programmatic dependent of the statistics pass, this
+    // kernel becomes resident on the SMs that pass leaves while it finishes;
+    // the wait returns once the pass has completed and its writes (the gains
+    // that setup_frame reads) are visible. Without a programmatic launch it
+    // returns at once.
+    griddep_wait();
+    // The next frame's statistics pass may launch now (when queued right
+    // behind this kernel): it sums its own raw frame on the SMs this pass
+    // leaves as it finishes, and waits for this pass's completion before its
+    // estimate touches the white balance state read here.
+    griddep_launch_dependents();
+    f = setup_frame<kLutSmem, false>(p, m);
+    waited = true;
+  };
 
   u64 acc[4] = {0, 0, 0, 0};  // linear R, G, B in 2^-20 units; saturated samples
   uint32_t phase = 0;
@@ -457,11 +478,13 @@ __global__ void __launch_bounds__(kThreads, kTileH == kTH ? 2 : 3)
     const auto before_c = [&] {
       if constexpr (kSharpen) request();
     };
-    run_tile<kMalvar, kSharpen, kLayout, kLutSmem, decltype(after_a), kOut, kTileH, decltype(before_c)>(
-        p, f, m, minmax, x0, ty * kTileH, use_tma != 0, &bar, phase, acc, after_a, before_c);
+    run_tile<kMalvar, kSharpen, kLayout, kLutSmem, decltype(after_a), kOut, kTileH, decltype(before_c),
+             decltype(wait_frame)>(p, f, m, minmax, x0, ty * kTileH, use_tma != 0, &bar, phase, acc, after_a, before_c,
+                                   wait_frame);
     ++done;
     tile = next_tile;  // written before run_tile's closing barrier
   }
+  wait_frame();  // a CTA without a tile still takes part in the flush
   flush_frame(p, f, acc, m.hist, red, &last, done, static_cast<unsigned int>(tiles));
 }
 
