@@ -59,8 +59,10 @@ def _compile(src: str, verbose: bool, checked: bool = False) -> str:
     if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
         return out
     # The checked build is for tests: its kernels are compiled with less
-    # scheduling effort (the checks make them large), not other arithmetic.
-    cmd = [NVCC, *ARCH, *COMMON, *(["-DISP_CHECKED", "-Xptxas", "-O1"] if checked else []), "-c", path, "-o", out]
+    # scheduling effort in ptxas (the checks make them large), not other
+    # arithmetic (no contraction either way, --fmad=false).
+    checked_flags = ["-DISP_CHECKED", "-Xptxas", "-O1"]
+    cmd = [NVCC, *ARCH, *COMMON, *(checked_flags if checked else []), "-c", path, "-o", out]
     if src.endswith(".cpp"):
         cmd[1:1] = ["-x", "cu"]
     if verbose and src.endswith(".cu"):
