@@ -1,6 +1,7 @@
 """Tracing: the library's host-side phases are NVTX ranges in the domain
 "holoscan.isp" (frame submission, the statistics and tile pass launches, host
-staging, batch build and replay, the converter and the view), seen by any
+staging, batch build and replay, the serving loop, the converter and the
+view), seen by any
 tool that NVTX loads. The tool here is tests/nvtx_probe.c, an NVTX injection
 library that records every range; each case runs in a child process so that
 NVTX loads it at the process's first NVTX call."""
@@ -128,3 +129,36 @@ def test_frame_phases_are_ranges(probe, tmp_path):
     direct = ("isp.batch.launch", [("isp.batch.build", []), ("isp.batch.enqueue", [])])
     replay = ("isp.batch.launch", [("isp.batch.build", []), ("isp.batch.replay", [])])
     assert trees == [frame, frame, host, direct, replay], json.dumps(trees)
+
+
+@pytest.mark.gpu
+def test_serving_loop_phases_are_ranges(probe, tmp_path):
+    """The server's worker marks each admission, each batch it launches (the
+    batch launch nested inside) and each batch it retires."""
+    lines = run_traced(probe, """
+        import numpy as np
+        import isp_b200
+        from isp_b200 import abi, scene
+
+        w, h = 256, 128
+        params = abi.IspParams(black_level=64.0, white_balance=abi.GRAY_WORLD, demosaic=abi.MALVAR, ccm=scene.CCM)
+        server = isp_b200.Server(max_batch=4, max_inflight=2, queue_depth=3, slots_per_stream=2)
+        sid = server.add_stream(params, w, h, abi.RAW10, 10, abi.GRBG, abi.RGB8)
+        server.start()
+        outs = []
+        for k in range(3):
+            counts = scene.mosaic_counts(w, h, abi.GRBG, 64.0, 1023, 10, 11 + k)
+            data, pitch = scene.pack(counts, abi.RAW10)
+            img = np.zeros((h, w, 3), np.uint8)
+            outs.append(img)
+            server.submit(sid, abi.RawFrame(data, w, h, pitch, abi.RAW10, 10, abi.GRBG), img)
+        server.drain(60.0)
+        assert server.stats()["completed"] == 3
+        server.close()
+    """, tmp_path)
+    trees = ranges_of(lines)
+    names = [n for n, _ in trees]
+    assert names.count("isp.server.admit") == 3, names
+    launches = [c for n, c in trees if n == "isp.server.launch"]
+    assert launches and all(c and all(k == "isp.batch.launch" for k, _ in c) for c in launches), json.dumps(trees)
+    assert names.count("isp.server.retire") == len(launches), names
