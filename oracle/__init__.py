@@ -80,6 +80,32 @@ def reference_available() -> bool:
     return os.path.exists(REF_SO)
 
 
+REF_VIEW_SO = os.path.join(_HERE, "_ref", "libview_ref_cuda.so")
+_ref_view = None
+
+
+def reference_view_available() -> bool:
+    return os.path.exists(REF_VIEW_SO)
+
+
+def reference_view_compose(raw_ptr: int, raw_pitch: int, width: int, height: int, fmt: int, bit_depth: int,
+                           black_level: float, rgb8_ptr: int, view_ptr: int, stream: int = 0) -> None:
+    """The reference demo's view kernel (view_op.cu, built for sm_100a into
+    oracle/_ref/libview_ref_cuda.so), launched as its operator launches it on
+    device buffers: the raw frame at raw_pitch, a packed RGB8 image and a
+    packed [H, 2W, 3] view. The checker of isp_b200_view_compose."""
+    global _ref_view
+    if _ref_view is None:
+        lib = C.CDLL(REF_VIEW_SO)
+        lib.ref_view_compose.argtypes = [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]
+        _ref_view = lib
+    rc = _ref_view.ref_view_compose(raw_ptr, raw_pitch, width, height, fmt, bit_depth, black_level, rgb8_ptr,
+                                    view_ptr, stream or None)
+    if rc != 0:
+        raise RuntimeError(f"reference view kernel launch failed: cudaError {rc}")
+
+
 REF_CUDA_SO = os.path.join(_HERE, "_ref", "libisp_ref_cuda.so")
 _ref_cuda = None
 

@@ -2,8 +2,10 @@
 raw mosaic as square-rooted gray on the left, the ISP's RGB8 image on the
 right. The C oracle is checked here against an independent numpy restatement
 (float32 arithmetic, one rounding per step); the GPU kernel, through
-isp_b200_view_compose, against the oracle byte for byte. Parity with the
-demo itself is unpinned: its source needs the Holoscan SDK to compile."""
+isp_b200_view_compose, against the oracle byte for byte, and against the
+demo's own view kernel: view_op.cu built from its source for sm_100a with
+the SDK's declarations stubbed (oracle/_ref/libview_ref_cuda.so, where the
+reference tree was present at build time), run on the same device buffers."""
 from __future__ import annotations
 
 import numpy as np
@@ -85,6 +87,27 @@ def test_view_kernel_matches_oracle(fmt, bits):
         want = oracle.view_compose(raw, black, rgb)
         assert np.array_equal(got[:, :6 * w].reshape(h, 2 * w, 3), want), (fmt, bits, w, h)
         assert (got[:, 6 * w:] == 0xAB).all(), "row padding was written"
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not oracle.reference_view_available(), reason="the reference view kernel is not built")
+@pytest.mark.parametrize("fmt,bits", FORMATS)
+def test_view_kernel_matches_the_demos_kernel(fmt, bits):
+    import torch
+
+    for w, h, black in ((3840, 2160, 64.0), (37, 11, 16.0), (1, 1, 0.0), (130, 9, 255.0 if bits > 8 else 17.0),
+                        (640, 480, float((1 << bits) - 2))):
+        raw = random_raw(fmt, bits, w, h, seed=3 * w + bits)
+        rgb = np.random.default_rng(w + 1).integers(0, 256, (h, w, 3), dtype=np.uint8)
+        d_raw = torch.from_numpy(raw.data).cuda()
+        d_rgb = torch.from_numpy(rgb.reshape(-1)).cuda()
+        ours = torch.full((h * 6 * w,), 0xAB, dtype=torch.uint8, device="cuda")
+        theirs = torch.full((h * 6 * w,), 0x5C, dtype=torch.uint8, device="cuda")
+        isp_b200.view_compose(raw.view(d_raw.data_ptr()), black, d_rgb.data_ptr(), 3 * w, ours.data_ptr(), 6 * w)
+        oracle.reference_view_compose(d_raw.data_ptr(), raw.pitch, w, h, fmt, bits, black, d_rgb.data_ptr(),
+                                      theirs.data_ptr())
+        torch.cuda.synchronize()
+        assert torch.equal(ours, theirs), (fmt, bits, w, h, black)
 
 
 def test_view_rejects():
