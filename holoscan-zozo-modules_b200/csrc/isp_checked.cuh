@@ -37,8 +37,8 @@ struct CheckRecord {
   uint4 sink[16];
 };
 
-// The record of spans that have none (null spans): an access through one is
-// refused and counted here rather than dereferencing null.
+// The record of spans built without one (Span(nullptr)): an access through
+// such a span is refused and counted here rather than dereferencing null.
 static __device__ CheckRecord g_unowned_check;
 
 static __device__ __noinline__ CheckRecord* check_failed(CheckRecord* rec, const void* at, size_t bytes,
@@ -94,10 +94,12 @@ struct Span {
   __host__ __device__ bool operator!=(std::nullptr_t) const { return p != nullptr; }
 };
 
-// A Span over `count` elements at ptr (null stays null), counting into rec.
+// A Span over `count` elements at ptr, counting into rec. A null ptr gives a
+// null span that still counts into rec: an access through it is refused and
+// reported like any other.
 template <class T>
 __host__ __device__ inline Span<T> make_span(T* ptr, size_t count, CheckRecord* rec) {
-  return ptr == nullptr ? Span<T>(nullptr) : Span<T>(ptr, ptr, ptr + count, rec);
+  return ptr == nullptr ? Span<T>(nullptr, nullptr, nullptr, rec) : Span<T>(ptr, ptr, ptr + count, rec);
 }
 // The same bytes viewed as U (for vector loads and stores, and carving).
 template <class U, class T>
